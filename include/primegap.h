@@ -1,0 +1,183 @@
+/*
+ * primegap.h -- C ABI of the B200 prime-gap search library (libprimegap.so).
+ *
+ * The library finds, for every m coprime to d in a window, the previous and
+ * next prime around the centre m*K, K = P#/d, and the merit of the gap
+ * between them.  It replaces the data plane of sethtroisi/prime-gap-gpu:
+ *
+ *   reference                                       replaced by
+ *   ----------------------------------------------  ------------------------------
+ *   test_runner_t ctor/dtor (miller_rabin.h:322-362)  pg_ctx_create / pg_ctx_destroy
+ *   test_runner_t::run_test (miller_rabin.h:364-408)  pg_prp_batch (host buffers)
+ *                                                     pg_prp_batch_device (device)
+ *   init_K + sieve prework (gap_common.cpp:60-65,     pg_job_create
+ *     gap_search_gpu.cpp:471-501)
+ *   per-X sieve pass (gap_search_gpu.cpp:570-755),    pg_sieve_interval
+ *     GPUSieve::run (sieve_small.h:40)
+ *   GPU batches + CPU overflow finishing              pg_search
+ *     (gpu_testing.cu:203-350, overflow.cpp:61-227)
+ *
+ * Conventions
+ *   - Every function returns PG_OK (0) or a negative PG_ERR_* code; nothing
+ *     calls exit().  pg_last_error() describes the last failure of the
+ *     calling thread.
+ *   - Numbers are little-endian arrays of uint32 words (the mpz_export order
+ *     -1 of miller_rabin.h:39-54).
+ *   - d must be even (gap_search_gpu.cpp:240, :269), so every m searched is
+ *     odd and every candidate N = m*K + X has X even.
+ *   - A context owns one CUDA stream on one device.  Use one context per host
+ *     thread; calls on the same context are serialised by the caller.
+ */
+#ifndef PRIMEGAP_H
+#define PRIMEGAP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PG_OK 0
+#define PG_ERR_ARG (-1)         /* invalid argument */
+#define PG_ERR_CUDA (-2)        /* CUDA runtime error */
+#define PG_ERR_UNSUPPORTED (-3) /* size outside the compiled kernels */
+#define PG_ERR_NOMEM (-4)       /* device or host allocation failed */
+#define PG_ERR_TIMEOUT (-5)     /* a bounded device wait gave up */
+#define PG_ERR_STATE (-6)       /* call made in the wrong state */
+
+/* largest operand, in 32-bit words, the PRP kernels accept */
+#define PG_MAX_WORDS 160
+
+typedef struct pg_ctx pg_ctx;
+typedef struct pg_job pg_job;
+
+/* ---------------------------------------------------------------- context */
+
+/* Creates a context on CUDA device `device` with its own stream.
+ * Replaces the resources test_runner_t allocates (miller_rabin.h:322-349). */
+int pg_ctx_create(int device, pg_ctx **out);
+int pg_ctx_destroy(pg_ctx *ctx);
+
+/* The context's cudaStream_t (as void *): every kernel of the context's
+ * calls is enqueued on it, so callers can time them with CUDA events. */
+void *pg_ctx_stream(pg_ctx *ctx);
+
+/* Text of the last error on this thread ("" if none). */
+const char *pg_last_error(void);
+
+/* Measured throughput of independent 32-bit integer multiply-adds on the
+ * context's device (instructions per second, whole GPU), from a register-only
+ * microbenchmark kernel.  No counterpart in the reference: it is the
+ * denominator of the PRP kernel's roofline.  Synchronous. */
+int pg_measure_imad_peak(pg_ctx *ctx, double *imad_per_second);
+
+/* Version string of the library. */
+const char *pg_version(void);
+
+/* ------------------------------------------------------------------- PRP */
+
+/* Strong probable-prime test of n numbers, each `words` LE uint32 words, in
+ * host memory; bases are the first `rounds` primes (2, 3, 5, ...).
+ * passed[i] = number of bases passed before the first failure, exactly the
+ * `passed` field of the reference (miller_rabin.h:216-270); the number is a
+ * probable prime iff passed[i] == rounds.  Even numbers and numbers < 3
+ * give 0.  Synchronous, like test_runner_t::run_test (miller_rabin.h:364). */
+int pg_prp_batch(pg_ctx *ctx, const uint32_t *limbs, uint32_t n, uint32_t words,
+                 uint32_t rounds, int32_t *passed);
+
+/* Same on device buffers, enqueued on `stream` (a cudaStream_t, or NULL for
+ * the context's stream); returns without waiting. */
+int pg_prp_batch_device(pg_ctx *ctx, const uint32_t *d_limbs, uint32_t n, uint32_t words,
+                        uint32_t rounds, int32_t *d_passed, void *stream);
+
+/* ------------------------------------------------------------------- jobs */
+
+typedef struct {
+    uint32_t p;            /* P of P# (-p), prime */
+    uint32_t d;            /* divisor (-d), even, divides P# */
+    uint32_t sl;           /* search radius: candidates X in [-sl, sl] are sieved */
+    uint64_t max_prime;    /* sieve limit: every prime <= max_prime (--max-prime * 1e6) */
+    uint64_t max_m_inc;    /* largest window later passed to pg_search / pg_sieve_interval */
+    uint64_t max_m;        /* largest m that will be searched (sizes the limbs) */
+    uint32_t rounds;       /* strong-PRP bases per accepted prime: 1 = base 2 only
+                              (the reference's ROUNDS, gpu_testing.cu:62); r > 1 confirms
+                              every base-2 probable prime with bases 3, 5, ... */
+    uint32_t small_limit;  /* primes <= small_limit are sieved per m in shared memory;
+                              0 = default (65536) */
+    uint32_t ext_window;   /* extension positions past sl tried in the first pass; 0 = 64 */
+    uint32_t flags;        /* PG_JOB_* */
+} pg_job_params;
+
+/* large-prime sieve: 0 = automatic, else force one method */
+#define PG_JOB_LARGE_STEP   0x1u   /* step every X for every prime */
+#define PG_JOB_LARGE_SEARCH 0x2u   /* modular search for the next hit */
+
+typedef struct {
+    uint32_t k_bits;          /* bits of K */
+    uint32_t limbs;           /* 32-bit words of the PRP operands */
+    uint32_t words_per_m;     /* uint32 words of one sieve row */
+    uint32_t side_capacity;   /* longest possible survivor list of one side */
+    uint64_t num_primes;      /* primes in (P, max_prime] */
+    uint64_t num_small;       /* of them (plus odd d-primes) sieved per m */
+    double k_log;             /* log(K), as _log (gap_common.cpp:44-48) */
+    double setup_seconds;     /* wall time of pg_job_create */
+    uint64_t device_bytes;    /* device memory held by the job */
+} pg_job_info;
+
+int pg_job_create(pg_ctx *ctx, const pg_job_params *params, pg_job **out);
+int pg_job_destroy(pg_job *job);
+int pg_job_get_info(const pg_job *job, pg_job_info *info);
+/* K as LE words; *nwords receives the count (call with out = NULL to size). */
+int pg_job_k_words(const pg_job *job, uint32_t *out, uint32_t *nwords);
+
+/* Number of m coprime to d in [m_start, m_start + m_inc). */
+uint64_t pg_count_m(uint64_t m_start, uint64_t m_inc, uint32_t d);
+
+/* Sieve of the window: for each m coprime to d in [m_start, m_start+m_inc)
+ * (ascending, written to ms) one row of words_per_m uint32, bit (Y + sl/2)
+ * set when m*K + 2Y has a prime factor <= max_prime.  Host buffers of
+ * pg_count_m(...) entries / rows.  This is sieve_interval_cpu's contract
+ * with both signs of X (the reference sieves X > 0 only). */
+int pg_sieve_interval(pg_job *job, uint64_t m_start, uint64_t m_inc, uint64_t *ms, uint32_t *bitmaps);
+
+/* Search forms */
+#define PG_SEARCH_PERSISTENT 0  /* one persistent kernel per window, device work queue */
+#define PG_SEARCH_PLAIN 1       /* one PRP launch per pass, host loop (the reference's shape) */
+
+typedef struct {
+    uint64_t m_count;         /* m searched */
+    uint64_t prp_tests;       /* strong base-2 tests executed */
+    uint64_t confirm_tests;   /* extra-base tests executed */
+    uint64_t extended_sides;  /* sides whose prime lay past sl */
+    uint32_t passes;          /* PRP launches (plain: one per pass) */
+    uint32_t relaunches;      /* continuation / re-search launches */
+    double sieve_ms;          /* device time of the sieve kernels */
+    double prp_ms;            /* device time of the PRP kernels, finalize and continuation */
+    double total_ms;          /* device time of the whole call, inputs already on the device */
+    double search_kernel_ms;  /* device time of the first PRP search launch(es) alone */
+    uint64_t kernel_launches; /* kernels of this library launched by the call */
+    uint64_t h2d_bytes;       /* host-to-device bytes copied by the call */
+    uint64_t d2h_bytes;       /* device-to-host bytes copied by the call */
+} pg_search_stats;
+
+/* Searches the window: for each m coprime to d (ascending; ms may be NULL)
+ * writes prev_gap[i] = m*K - prevprime(m*K) and next_gap[i] =
+ * nextprime(m*K) - m*K.  Host arrays of pg_count_m(...) entries.  Primes
+ * past sl are found on the device (no CPU fallback). */
+int pg_search(pg_job *job, uint64_t m_start, uint64_t m_inc, int form,
+              uint64_t *ms, uint32_t *prev_gap, uint32_t *next_gap, pg_search_stats *stats);
+
+/* Merit of a gap as overflow.cpp:162: gap / (k_log + log(m)). */
+double pg_merit(double k_log, uint64_t m, uint64_t gap);
+
+/* Record line of overflow.cpp:180-182: "{gap} {merit:.3f} {m} * {P}# / {D} - {prev}".
+ * Returns the length written (excluding NUL), or a negative error. */
+int pg_format_record(char *buf, size_t buflen, uint64_t gap, double merit, uint64_t m,
+                     uint32_t p, uint32_t d, uint64_t prev_gap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PRIMEGAP_H */

@@ -1,0 +1,333 @@
+"""prime-gap-gpu_b200: B200 prime-gap search behind the C ABI of libprimegap.so.
+
+Python mirror of the reference's interfaces for the hot path:
+
+  TestRunner(n, rounds).run_test(active, tests, results)
+      test_runner_t<params> (miller_rabin.h:296-409): strong PRP of a batch,
+      results[i] = 1 if tests[i] passed every base, 0 otherwise.
+  Job(p, d, sl, max_prime, ...)
+      K = P#/d and the sieve tables (init_K gap_common.cpp:60-65, the sieve
+      prework gap_search_gpu.cpp:471-501), resident on the device.
+  Job.sieve_interval(m_start, m_inc)
+      the per-m sieve rows (sieve_interval_cpu's contract, both signs of X).
+  Job.search(m_start, m_inc, form)
+      previous/next prime gap of every m coprime to d, found on the device
+      (the GPU batches of gpu_testing.cu:203-350 plus the CPU overflow
+      finishing of overflow.cpp:145-188).
+  merit(), format_record(), records()
+      overflow.cpp:162-188.
+
+There is no CPU fallback: importing this package loads libprimegap.so and
+raises if it is missing or was built without the symbols declared in
+include/primegap.h.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import math
+import pathlib
+
+import numpy as np
+
+PKG_DIR = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "build" / "libprimegap.so"
+
+PG_OK = 0
+PG_SEARCH_PERSISTENT = 0
+PG_SEARCH_PLAIN = 1
+PG_MAX_WORDS = 160
+PG_JOB_LARGE_STEP = 0x1
+PG_JOB_LARGE_SEARCH = 0x2
+
+# every symbol include/primegap.h declares
+EXPORTS = (
+    "pg_ctx_create", "pg_ctx_destroy", "pg_ctx_stream", "pg_last_error", "pg_version", "pg_measure_imad_peak",
+    "pg_prp_batch", "pg_prp_batch_device",
+    "pg_job_create", "pg_job_destroy", "pg_job_get_info", "pg_job_k_words",
+    "pg_count_m", "pg_sieve_interval", "pg_search", "pg_merit", "pg_format_record",
+)
+
+
+class PrimeGapError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libprimegap error {code}: {msg}")
+        self.code = code
+
+
+class JobParams(ctypes.Structure):
+    _fields_ = [
+        ("p", ctypes.c_uint32), ("d", ctypes.c_uint32), ("sl", ctypes.c_uint32),
+        ("max_prime", ctypes.c_uint64), ("max_m_inc", ctypes.c_uint64), ("max_m", ctypes.c_uint64),
+        ("rounds", ctypes.c_uint32), ("small_limit", ctypes.c_uint32),
+        ("ext_window", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+    ]
+
+
+class JobInfo(ctypes.Structure):
+    _fields_ = [
+        ("k_bits", ctypes.c_uint32), ("limbs", ctypes.c_uint32), ("words_per_m", ctypes.c_uint32),
+        ("side_capacity", ctypes.c_uint32), ("num_primes", ctypes.c_uint64), ("num_small", ctypes.c_uint64),
+        ("k_log", ctypes.c_double), ("setup_seconds", ctypes.c_double), ("device_bytes", ctypes.c_uint64),
+    ]
+
+
+class SearchStats(ctypes.Structure):
+    _fields_ = [
+        ("m_count", ctypes.c_uint64), ("prp_tests", ctypes.c_uint64), ("confirm_tests", ctypes.c_uint64),
+        ("extended_sides", ctypes.c_uint64), ("passes", ctypes.c_uint32), ("relaunches", ctypes.c_uint32),
+        ("sieve_ms", ctypes.c_double), ("prp_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+        ("search_kernel_ms", ctypes.c_double), ("kernel_launches", ctypes.c_uint64),
+        ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+def _load() -> ctypes.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python {PKG_DIR / 'build.py'}` "
+                          "(there is no CPU fallback)")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    missing = [s for s in EXPORTS if not hasattr(lib, s)]
+    if missing:
+        raise ImportError(f"{LIB_PATH} lacks {missing}")
+    vp, u32, u64, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
+    P32, P64, PI32 = ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int32)
+    lib.pg_ctx_create.argtypes = [i32, ctypes.POINTER(vp)]
+    lib.pg_ctx_destroy.argtypes = [vp]
+    lib.pg_ctx_stream.restype = vp
+    lib.pg_ctx_stream.argtypes = [vp]
+    lib.pg_measure_imad_peak.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    lib.pg_last_error.restype = ctypes.c_char_p
+    lib.pg_version.restype = ctypes.c_char_p
+    lib.pg_prp_batch.argtypes = [vp, P32, u32, u32, u32, PI32]
+    lib.pg_prp_batch_device.argtypes = [vp, vp, u32, u32, u32, vp, vp]
+    lib.pg_job_create.argtypes = [vp, ctypes.POINTER(JobParams), ctypes.POINTER(vp)]
+    lib.pg_job_destroy.argtypes = [vp]
+    lib.pg_job_get_info.argtypes = [vp, ctypes.POINTER(JobInfo)]
+    lib.pg_job_k_words.argtypes = [vp, P32, P32]
+    lib.pg_count_m.restype = u64
+    lib.pg_count_m.argtypes = [u64, u64, u32]
+    lib.pg_sieve_interval.argtypes = [vp, u64, u64, P64, P32]
+    lib.pg_search.argtypes = [vp, u64, u64, i32, P64, P32, P32, ctypes.POINTER(SearchStats)]
+    lib.pg_merit.restype = ctypes.c_double
+    lib.pg_merit.argtypes = [ctypes.c_double, u64, u64]
+    lib.pg_format_record.argtypes = [ctypes.c_char_p, ctypes.c_size_t, u64, ctypes.c_double, u64, u32, u32, u64]
+    return lib
+
+
+lib = _load()
+
+
+def _check(rc: int) -> int:
+    if rc < 0:
+        raise PrimeGapError(rc, lib.pg_last_error().decode())
+    return rc
+
+
+def _p32(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+
+
+def _p64(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+
+def version() -> str:
+    return lib.pg_version().decode()
+
+
+def count_m(m_start: int, m_inc: int, d: int) -> int:
+    """m coprime to d in [m_start, m_start + m_inc) (count_num_m, gap_common.cpp:170-206)."""
+    return int(lib.pg_count_m(m_start, m_inc, d))
+
+
+def int_to_words(n: int, nwords: int) -> np.ndarray:
+    return np.frombuffer(n.to_bytes(nwords * 4, "little"), dtype=np.uint32)
+
+
+class Context:
+    """A CUDA device and stream (the resources of test_runner_t's constructor)."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        _check(lib.pg_ctx_create(device, ctypes.byref(h)))
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream_ptr(self) -> int:
+        """The context's cudaStream_t, e.g. for torch.cuda.ExternalStream."""
+        return int(lib.pg_ctx_stream(self._h) or 0)
+
+    def imad_peak(self) -> float:
+        """Measured 32-bit integer multiply-adds per second of the whole device."""
+        v = ctypes.c_double(0)
+        _check(lib.pg_measure_imad_peak(self._h, ctypes.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.pg_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def prp_words(self, words: np.ndarray, rounds: int = 1) -> np.ndarray:
+        """Bases passed per row of a (n, w) uint32 array of LE words."""
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        n, w = words.shape
+        out = np.zeros(n, dtype=np.int32)
+        _check(lib.pg_prp_batch(self._h, _p32(words), n, w, rounds,
+                                out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+        return out
+
+    def prp(self, numbers, rounds: int = 1) -> np.ndarray:
+        numbers = [int(x) for x in numbers]
+        if not numbers:
+            return np.zeros(0, dtype=np.int32)
+        w = max(1, max((x.bit_length() + 31) // 32 for x in numbers))
+        arr = np.stack([int_to_words(x, w) for x in numbers])
+        return self.prp_words(arr, rounds)
+
+
+class TestRunner:
+    """Drop-in for test_runner_t<params> (miller_rabin.h:296-409).
+
+    run_test(active, tests, results): tests are Python ints (the mpz_t
+    batch), only the first `active` are computed, results[i] is set to
+    (bases passed == rounds) for every i < len(tests) as the reference does
+    (entries past `active` get 0 here instead of stale data).
+    """
+    __test__ = False  # not a pytest class
+
+    def __init__(self, n: int, rounds: int = 1, device: int = 0, ctx: Context | None = None):
+        self.n, self.rounds = n, rounds
+        self.ctx = ctx or Context(device)
+
+    def run_test(self, active: int, tests, results) -> None:
+        if len(tests) == 0:
+            return
+        if len(tests) > self.n:
+            raise ValueError(f"tests({len(tests)}) > n({self.n})")
+        to_run = min(active, len(tests))
+        for i in range(to_run):
+            t = int(tests[i])
+            if t <= 1 or t % 2 == 0:
+                raise ValueError("candidates must be odd and > 1")
+        passed = self.ctx.prp(list(tests[:to_run]), self.rounds) if to_run else []
+        for i in range(len(tests)):
+            results[i] = int(i < to_run and passed[i] == self.rounds)
+
+
+@dataclasses.dataclass
+class SearchResult:
+    ms: np.ndarray
+    prev_gap: np.ndarray
+    next_gap: np.ndarray
+    stats: dict
+
+
+class Job:
+    """K = P#/d, the sieve tables and the window buffers, resident on one device."""
+
+    def __init__(self, p: int, d: int, sl: int, max_prime: int, max_m_inc: int, max_m: int,
+                 rounds: int = 1, small_limit: int = 0, ext_window: int = 0, flags: int = 0,
+                 ctx: Context | None = None, device: int = 0):
+        self.ctx = ctx or Context(device)
+        self.params = JobParams(p, d, sl, max_prime, max_m_inc, max_m, rounds, small_limit, ext_window, flags)
+        h = ctypes.c_void_p()
+        _check(lib.pg_job_create(self.ctx.handle, ctypes.byref(self.params), ctypes.byref(h)))
+        self._h = h
+        info = JobInfo()
+        _check(lib.pg_job_get_info(self._h, ctypes.byref(info)))
+        self.info = {f: getattr(info, f) for f, _ in info._fields_}
+        self.p, self.d, self.sl, self.max_prime = p, d, sl, max_prime
+        self.sly = sl // 2
+        self.k_log = info.k_log
+        nw = ctypes.c_uint32(0)
+        _check(lib.pg_job_k_words(self._h, None, ctypes.byref(nw)))
+        kw = np.zeros(nw.value, dtype=np.uint32)
+        _check(lib.pg_job_k_words(self._h, _p32(kw), ctypes.byref(nw)))
+        self.K = int.from_bytes(kw.tobytes(), "little")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.pg_job_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def words_per_m(self) -> int:
+        return self.info["words_per_m"]
+
+    def sieve_interval(self, m_start: int, m_inc: int):
+        """(ms, rows): rows[i] bit (Y + sl//2) set when ms[i]*K + 2Y has a factor <= max_prime."""
+        n = count_m(m_start, m_inc, self.d)
+        ms = np.zeros(n, dtype=np.uint64)
+        rows = np.zeros((n, self.words_per_m), dtype=np.uint32)
+        _check(lib.pg_sieve_interval(self._h, m_start, m_inc, _p64(ms), _p32(rows)))
+        return ms, rows
+
+    def search(self, m_start: int, m_inc: int, form: int = PG_SEARCH_PERSISTENT) -> SearchResult:
+        n = count_m(m_start, m_inc, self.d)
+        ms = np.zeros(n, dtype=np.uint64)
+        prev = np.zeros(n, dtype=np.uint32)
+        nxt = np.zeros(n, dtype=np.uint32)
+        st = SearchStats()
+        _check(lib.pg_search(self._h, m_start, m_inc, form, _p64(ms), _p32(prev), _p32(nxt), ctypes.byref(st)))
+        return SearchResult(ms, prev, nxt, st.as_dict())
+
+    def merits(self, res: SearchResult) -> np.ndarray:
+        return np.array([merit(self.k_log, int(m), int(a) + int(b))
+                         for m, a, b in zip(res.ms, res.prev_gap, res.next_gap)])
+
+    def records(self, res: SearchResult, min_merit: float) -> list[str]:
+        """Record lines of every gap with merit > min_merit (overflow.cpp:162-188, strict >)."""
+        out = []
+        for m, pg, ng in zip(res.ms, res.prev_gap, res.next_gap):
+            gap = int(pg) + int(ng)
+            mer = merit(self.k_log, int(m), gap)
+            if mer > min_merit:
+                out.append(format_record(gap, mer, int(m), self.p, self.d, int(pg)))
+        return out
+
+
+def merit(k_log: float, m: int, gap: int) -> float:
+    """gap / (K_log + log(m)) (overflow.cpp:162)."""
+    return lib.pg_merit(k_log, m, gap)
+
+
+def format_record(gap: int, merit_value: float, m: int, p: int, d: int, prev_gap: int) -> str:
+    """"{gap} {merit:.3f} {m} * {P}# / {D} - {prev_gap}" (overflow.cpp:180-182)."""
+    buf = ctypes.create_string_buffer(256)
+    n = _check(lib.pg_format_record(buf, 256, gap, merit_value, m, p, d, prev_gap))
+    return buf.raw[:n].decode()
+
+
+def k_log_of(K: int) -> float:
+    """log(K) exactly as _log (gap_common.cpp:44-48): 53-bit truncated mantissa."""
+    b = K.bit_length()
+    top = K >> (b - 53) if b > 53 else K << (53 - b)
+    return math.log(top / 2.0 ** 53) + math.log(2.0) * b

@@ -1,0 +1,102 @@
+// pg_internal.h -- declarations shared by the kernels (pg_kernels.cu) and the
+// host side of the C ABI (pg_api.cu).  Not part of the public interface.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "../../include/primegap.h"
+
+namespace pg {
+
+constexpr uint32_t NOT_FOUND = 0xffffffffu;
+constexpr uint32_t TRIAL_PRIMES = 256;  // odd primes tried on positions past sl
+
+// Arguments of the search kernels.  K travels in the parameter space (a
+// broadcast constant bank read) so building m*K + X costs no memory traffic.
+struct SearchArgs {
+    uint32_t K[PG_MAX_WORDS];
+    uint32_t kwords;
+    uint32_t sly;            // sl / 2; positions Y in [-sly, sly], X = 2Y
+    uint32_t cap;            // list capacity per side
+    uint32_t n_act;          // active sides in this launch
+    uint32_t kspan;          // items per active side in this launch
+    uint32_t ext_max;        // extension positions allowed past sly (absolute)
+    uint32_t ntrial;         // trial primes for extension positions
+    uint32_t rounds;         // confirmation: total bases
+    const uint64_t *ms;      // m of each m index
+    const uint16_t *lists;   // [2M][cap] |Y| of the survivors, nearest first
+    const uint32_t *counts;  // [2M] survivors per side
+    const uint32_t *act;     // active side ids
+    const uint32_t *k_start; // [2M] first item of each side
+    const uint32_t *max_count;  // device scalar: longest list (bounds the queue)
+    uint32_t *found_k;       // [2M] item index of the first probable prime
+    unsigned long long *next_item;  // work-queue head
+    unsigned long long *tests;      // PRP tests executed
+    const uint32_t *trial_q;   // [TRIAL_PRIMES] 3, 5, 7, ...
+    const uint32_t *trial_r;   // [TRIAL_PRIMES] (-(K mod q)/2) mod q
+};
+
+// Arguments of the sieve kernels for one window.
+struct SieveArgs {
+    uint32_t sly;
+    uint32_t words;          // words per row
+    uint32_t cap;
+    uint64_t m0;             // first odd m of the window
+    uint64_t nodd;           // odd m in the window
+    uint32_t nm;             // coprime m in the window
+    const uint64_t *ms;      // [nm]
+    const int32_t *rank;     // [nodd] index among coprime m, -1 if gcd(m, d) > 1
+    uint32_t *bitmaps;       // [nm][words]
+    const uint32_t *wheel;   // [words] Y = 0 and q | Y for q | K
+    // small primes sieved per m: q, r = (-(K mod q)/2) mod q, floor(2^64/q)
+    const uint32_t *sq;
+    const uint32_t *sr;
+    const uint64_t *sbar;
+    uint32_t nsmall;
+    uint16_t *lists;
+    uint32_t *counts;
+    uint32_t *max_count;
+};
+
+struct LargeArgs {
+    uint32_t sly;
+    uint32_t words;
+    uint64_t m0;
+    uint64_t nodd;
+    const int32_t *rank;
+    uint32_t *bitmaps;
+    uint64_t np;
+    const void *p;      // uint32 or uint64 primes
+    const void *cinv;   // K^-1 mod p, same type
+    const void *c;      // K mod p, same type
+};
+
+// --- launchers (pg_kernels.cu); all enqueue on `st` and return cudaError_t
+cudaError_t launch_prime_count(uint64_t v_first, uint64_t limit, const uint32_t *base, uint32_t nbase,
+                               uint32_t nseg, uint32_t *seg_counts, cudaStream_t st);
+cudaError_t launch_prime_write(uint64_t v_first, uint64_t limit, const uint32_t *base, uint32_t nbase,
+                               uint32_t nseg, const uint64_t *seg_offsets, void *out, bool wide, cudaStream_t st);
+cudaError_t launch_prime_tables(const uint32_t *K, uint32_t kwords, uint64_t np, const void *p, void *c,
+                                void *cinv, bool wide, cudaStream_t st);
+cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, int method, cudaStream_t st);
+cudaError_t launch_sieve_small(const SieveArgs &a, bool compact, cudaStream_t st);
+cudaError_t launch_prp_batch(uint32_t L, const uint32_t *cand, uint32_t words, uint32_t n, uint32_t rounds,
+                             int32_t *out, cudaStream_t st);
+cudaError_t launch_search_persistent(uint32_t L, const SearchArgs &a, int grid, cudaStream_t st);
+cudaError_t launch_search_plain(uint32_t L, const SearchArgs &a, uint32_t *k_next, cudaStream_t st);
+cudaError_t launch_compact_active(const uint32_t *act_in, uint32_t n_in, const uint32_t *found_k,
+                                  const uint32_t *k_next, const uint32_t *counts, uint32_t ext_max,
+                                  uint32_t *act_out, uint32_t *n_out, cudaStream_t st);
+cudaError_t launch_finalize(uint32_t L, const SearchArgs &a, uint32_t nsides, uint32_t *gaps,
+                            uint32_t *redo, uint32_t *n_redo, unsigned long long *confirm_tests,
+                            uint32_t *k_start_rw, cudaStream_t st);
+cudaError_t launch_iota(uint32_t *out, uint32_t n, cudaStream_t st);
+cudaError_t launch_imad_peak(int grid, uint32_t iters, uint32_t *sink, cudaStream_t st);
+int search_grid(uint32_t L, int device);
+bool supported_limbs(uint32_t L);
+uint32_t pick_limbs(uint32_t words);  // smallest compiled L >= words, 0 if none
+
+}  // namespace pg

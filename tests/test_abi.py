@@ -1,0 +1,73 @@
+"""The C-ABI library loads and exports every declared symbol; host-only helpers
+(no GPU needed) agree with the oracle and the reference's formulas."""
+from __future__ import annotations
+
+import math
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+
+def declared_functions() -> list[str]:
+    text = (ROOT / "include" / "primegap.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pg_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_boundary():
+    fns = declared_functions()
+    for f in ("pg_ctx_create", "pg_prp_batch", "pg_job_create", "pg_sieve_interval", "pg_search"):
+        assert f in fns
+
+
+def test_library_exports_every_declared_symbol(pg):
+    out = subprocess.run(["nm", "-D", "--defined-only", str(pg.LIB_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = set(re.findall(r" T (pg_\w+)", out))
+    missing = [f for f in declared_functions() if f not in exported]
+    assert not missing, missing
+    assert set(declared_functions()) <= set(pg.EXPORTS)
+
+
+@pytest.mark.parametrize("m_start,m_inc,d", [(10_000_000, 10_000, 2310), (1_000_000, 200_000, 2190),
+                                             (1, 100_000, 2190), (999_999, 12_345, 210), (7, 1, 30)])
+def test_count_m_matches_oracle(pg, oracle, m_start, m_inc, d):
+    assert pg.count_m(m_start, m_inc, d) == len(oracle.coprime_ms(m_start, m_inc, d))
+
+
+def test_counts_of_the_benchmark_windows(pg):
+    # survey figures for the configurations: 2,079 / 52,604 / 11,429 / 26,300 m
+    assert pg.count_m(10_000_000, 10_000, 2310) == 2079
+    assert pg.count_m(1_000_000, 200_000, 2190) == 52604
+    assert pg.count_m(1_000_000, 50_000, 210) == 11429
+    assert pg.count_m(1, 100_000, 2190) == 26300
+
+
+@pytest.mark.parametrize("P,d", [(337, 2310), (503, 2190), (907, 210), (3001, 2190), (151, 2310)])
+def test_k_log_matches_gmp(pg, oracle, P, d):
+    with oracle.Job(P, d, 100, 10_000, threads=1) as j:
+        assert pg.k_log_of(j.K) == j.K_log
+
+
+def test_merit_formula(pg):
+    k_log = 303.87395620173214
+    for m, gap in [(10_000_003, 692), (1_000_001, 15000), (1, 2)]:
+        assert pg.merit(k_log, m, gap) == gap / (k_log + math.log(m))
+
+
+def test_record_format(pg):
+    line = pg.format_record(15234, 22.51849, 1000003, 503, 2190, 7342)
+    assert line == "15234 22.518 1000003 * 503# / 2190 - 7342"
+    # parses with the record regex of misc/record_check.py:430-434
+    assert re.match(r"(\d+)\s+(\d+\.\d+)\s+(\d+)\s*\*\s*(\d+)#\s*/\s*(\d+)\s*-\s*(\d+)", line)
+
+
+def test_context_without_gpu_reports_an_error(pg):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(pg.PrimeGapError):
+        pg.Context(0)

@@ -1,0 +1,112 @@
+"""Full search (pg_search): gaps, records and PRP accounting against GMP and the oracle."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _job(pg, g, **kw):
+    return pg.Job(g["P"], g["d"], g["sl"], g["max_prime"], max_m_inc=g["m_inc"],
+                  max_m=g["m_start"] + g["m_inc"], **kw)
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_cfg1_full_window(pg, form):
+    """P=337, d=2310, m in [1e7, 1e7+1e4), SL 7500, primes <= 1e8: every gap equals GMP's."""
+    g = golden("gaps_cfg1.json")
+    with _job(pg, g) as job:
+        assert job.k_log == g["k_log"]
+        res = job.search(g["m_start"], g["m_inc"], form)
+        assert [int(m) for m in res.ms] == g["ms"]
+        assert list(res.prev_gap) == g["prev_gap"]
+        assert list(res.next_gap) == g["next_gap"]
+        assert job.records(res, g["min_merit"]) == g["records"]
+        st = res.stats
+        assert st["m_count"] == 2079 and st["prp_tests"] > 2 * 2079
+        if form == 1:
+            assert st["passes"] > 10
+
+
+@pytest.mark.parametrize("name", ["gaps_cfg2.json", "gaps_cfg3.json"])
+def test_config_windows_against_gmp(pg, name):
+    """The whole P=503 (primes <= 2e9) / P=907 (primes <= 1e10) windows; the GMP-sampled m must match."""
+    g = golden(name)
+    with _job(pg, g) as job:
+        res = job.search(g["m_start"], g["m_inc"])
+    pos = {int(m): i for i, m in enumerate(res.ms)}
+    for m, a, b in zip(g["ms"], g["prev_gap"], g["next_gap"]):
+        i = pos[m]
+        assert (int(res.prev_gap[i]), int(res.next_gap[i])) == (a, b), m
+    assert (res.prev_gap > 0).all() and (res.next_gap > 0).all()
+    assert (res.prev_gap % 2 == 0).all() and (res.next_gap % 2 == 0).all()
+
+
+def test_cfg2_sieve_matches_oracle_on_a_sample(pg, oracle):
+    g = golden("gaps_cfg2.json")
+    with _job(pg, g) as job:
+        ms, rows = job.sieve_interval(g["m_start"], 400)
+    with oracle.Job(g["P"], g["d"], g["sl"], g["max_prime"]) as oj:
+        sel = np.arange(0, len(ms), 13)
+        want = oj.sieve_m(ms[sel])
+    assert np.array_equal(rows[sel], want)
+
+
+def test_plain_equals_persistent(pg):
+    with pg.Job(503, 2190, 10_000, 50_000_000, max_m_inc=20_000, max_m=2_000_000) as job:
+        a = job.search(1_000_000, 20_000, pg.PG_SEARCH_PERSISTENT)
+        b = job.search(1_000_000, 20_000, pg.PG_SEARCH_PLAIN)
+    assert np.array_equal(a.prev_gap, b.prev_gap) and np.array_equal(a.next_gap, b.next_gap)
+    assert b.stats["passes"] > a.stats["passes"]
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_continuation_past_sl(pg, oracle, form):
+    """SL far below the typical gap: most sides continue on the device past SL."""
+    m_start, m_inc = 10_000_000, 600
+    with pg.Job(337, 2310, 60, 1_000_000, max_m_inc=m_inc, max_m=m_start + m_inc) as job:
+        res = job.search(m_start, m_inc, form)
+    with oracle.Job(337, 2310, 60, 1_000_000) as oj:
+        prev, nxt = oj.gmp_gaps(res.ms)
+    assert np.array_equal(res.prev_gap, prev) and np.array_equal(res.next_gap, nxt)
+    assert res.stats["extended_sides"] > 0 or res.stats["relaunches"] == 0
+
+
+def test_confirmation_rounds(pg, oracle):
+    m_start, m_inc = 10_000_000, 1_000
+    with pg.Job(337, 2310, 7_500, 5_000_000, max_m_inc=m_inc, max_m=m_start + m_inc, rounds=3) as job:
+        res = job.search(m_start, m_inc)
+    with oracle.Job(337, 2310, 7_500, 5_000_000) as oj:
+        prev, nxt, _, _ = oj.search(res.ms, 3)
+    assert np.array_equal(res.prev_gap, prev) and np.array_equal(res.next_gap, nxt)
+    assert res.stats["confirm_tests"] == 2 * 2 * len(res.ms)
+
+
+def test_search_matches_oracle_search_and_test_count(pg, oracle):
+    """Same survivors, same verdicts: the persistent form never tests fewer than the oracle."""
+    m_start, m_inc = 1_000_000, 2_000
+    with pg.Job(503, 2190, 10_000, 10_000_000, max_m_inc=m_inc, max_m=m_start + m_inc) as job:
+        res = job.search(m_start, m_inc, pg.PG_SEARCH_PLAIN)
+    with oracle.Job(503, 2190, 10_000, 10_000_000) as oj:
+        prev, nxt, _, tests = oj.search(res.ms, 1)
+    assert np.array_equal(res.prev_gap, prev) and np.array_equal(res.next_gap, nxt)
+    assert res.stats["prp_tests"] == tests  # the plain form tests exactly the needed candidates
+
+
+def test_odd_start_and_small_windows(pg, oracle):
+    with pg.Job(151, 2310, 800, 1_000_000, max_m_inc=500, max_m=10**12) as job, \
+            oracle.Job(151, 2310, 800, 1_000_000) as oj:
+        for m_start, m_inc in [(956_702_000_001, 500), (1, 30), (13, 4), (3, 1), (999_999_999_999, 1)]:
+            res = job.search(m_start, m_inc)
+            prev, nxt = oj.gmp_gaps(res.ms)
+            assert np.array_equal(res.prev_gap, prev) and np.array_equal(res.next_gap, nxt)
+
+
+def test_repeat_is_deterministic(pg):
+    with pg.Job(337, 2310, 7_500, 1_000_000, max_m_inc=3_000, max_m=2 * 10**7) as job:
+        a = job.search(10_000_000, 3_000)
+        b = job.search(10_000_000, 3_000)
+    assert np.array_equal(a.prev_gap, b.prev_gap) and np.array_equal(a.next_gap, b.next_gap)

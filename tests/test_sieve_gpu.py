@@ -1,0 +1,77 @@
+"""Sieve kernels (pg_sieve_interval) bit for bit against the oracle."""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _job(pg, P, d, sl, limit, m_start, m_inc, **kw):
+    return pg.Job(P, d, sl, limit, max_m_inc=m_inc, max_m=m_start + m_inc, **kw)
+
+
+def test_golden_rows(pg):
+    g = golden("sieve_rows.json")
+    with _job(pg, g["P"], g["d"], g["sl"], g["max_prime"], g["m_start"], g["m_inc"]) as job:
+        ms, rows = job.sieve_interval(g["m_start"], g["m_inc"])
+    assert [int(m) for m in ms] == g["ms"]
+    assert rows.shape[1] == g["words_per_m"]
+    assert [hashlib.sha256(r.tobytes()).hexdigest() for r in rows] == g["row_sha256"]
+
+
+@pytest.mark.parametrize("P,d,sl,limit,m_start,m_inc,small", [
+    (503, 2190, 10_000, 20_000_000, 1_000_000, 3_000, 0),        # large-prime kernel from 65536
+    (503, 2190, 10_000, 20_000_000, 1_000_000, 3_000, 1_000),    # most primes in the large kernel
+    (337, 2310, 7_500, 60_000, 10_000_000, 4_000, 0),            # limit below the small split
+    (907, 210, 18_000, 5_000_000, 1_000_000, 1_000, 4_096),
+    (3001, 2190, 40_000, 3_000_000, 1, 600, 0),                  # m from 1, 4231-bit K
+    (151, 2310, 1_234, 1_000_000, 956_702_000_001, 5_000, 0),    # odd m_start, m above 2^32
+    (337, 2310, 3, 100_000, 10_000_000, 500, 0),                 # SL = 3: one position per side
+])
+def test_rows_match_oracle(pg, oracle, P, d, sl, limit, m_start, m_inc, small):
+    with _job(pg, P, d, sl, limit, m_start, m_inc, small_limit=small) as job:
+        ms, rows = job.sieve_interval(m_start, m_inc)
+    with oracle.Job(P, d, sl, limit) as oj:
+        assert np.array_equal(ms, oracle.coprime_ms(m_start, m_inc, d))
+        want = oj.sieve_m(ms)
+    assert np.array_equal(rows, want)
+
+
+def test_wide_primes_above_2_32(pg, oracle):
+    """max_prime above 2^32: 64-bit prime tables and residues."""
+    P, d, sl, limit, m_start, m_inc = 503, 2190, 4_000, 4_300_000_000, 1_000_000, 60
+    with _job(pg, P, d, sl, limit, m_start, m_inc) as job:
+        ms, rows = job.sieve_interval(m_start, m_inc)
+        assert job.info["num_primes"] > 200_000_000
+    with oracle.Job(P, d, sl, limit) as oj:
+        want = oj.sieve_m(ms)
+    assert np.array_equal(rows, want)
+
+
+def test_windows_reuse_one_job(pg, oracle):
+    P, d, sl, limit = 337, 2310, 2_000, 2_000_000
+    with pg.Job(P, d, sl, limit, max_m_inc=2_000, max_m=10**8) as job, oracle.Job(P, d, sl, limit) as oj:
+        for m_start, m_inc in [(10_000_000, 2_000), (10_002_000, 1_000), (20_000_001, 7), (99_998_000, 2_000)]:
+            ms, rows = job.sieve_interval(m_start, m_inc)
+            assert np.array_equal(rows, oj.sieve_m(ms))
+
+
+def test_window_too_large_is_an_error(pg):
+    with pg.Job(337, 2310, 100, 10_000, max_m_inc=100, max_m=10**8) as job:
+        with pytest.raises(pg.PrimeGapError):
+            job.sieve_interval(10_000_000, 101)
+        with pytest.raises(pg.PrimeGapError):
+            job.sieve_interval(10**8, 100)
+
+
+@pytest.mark.parametrize("bad", [dict(p=338), dict(d=15), dict(d=2 * 1009), dict(sl=1), dict(sl=300_000)])
+def test_bad_jobs_are_errors(pg, bad):
+    kw = dict(p=337, d=2310, sl=100, max_prime=10_000, max_m_inc=100, max_m=10**8)
+    kw.update(bad)
+    with pytest.raises(pg.PrimeGapError):
+        pg.Job(**kw)
