@@ -1,0 +1,360 @@
+"""Benchmark of the prime-gap search path on B200 (one JSON line on stdout).
+
+Workload (the single-GPU configuration the metric is quoted on): P=503,
+d=2190, every m in [1,000,000, 1,200,000) coprime to d (52,604 m), candidates
+N = m*503#/2190 + X for X in [-10,000, 10,000] sieved by every prime <= 2e9,
+strong base-2 PRP outward from X = 0 for the previous and the next prime,
+records of merit > 22.  A step is one search of that window (sieve + PRP +
+finalize), the inputs being the window bounds; the prime tables (98 M primes,
+786 MB with their K^-1 residues) are read again by every step, far more than
+the 126 MB L2, so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank searches its own window of 200,000 m (weak scaling,
+no data-path collective); the reported time is the max over ranks.
+`--impl reference` times the reference's CPU path (the oracle's restatement,
+the reference itself does not build here) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = dict(p=503, d=2190, m_start=1_000_000, m_inc=200_000, sl=10_000, max_prime=2_000_000_000,
+                min_merit=22.0)
+# distinct windows of 200,000 m per rank, all m < 2^21 so every rank runs the same 22-word operands
+RANK_STARTS = [1_000_000, 1_200_000, 1_400_000, 1_600_000, 1_800_000, 800_000, 600_000, 400_000]
+METRIC = "m/sec searched (prev+next prime of every m, bit-exact vs GMP)"
+WINDOW_BITS = 5  # the reference's window for <= 1024-bit operands (gpu_testing.cu:50)
+
+
+def workload_name(start: int, inc: int) -> str:
+    return (f"P=503 d=2190 m in [{start:,}, {start + inc:,}) coprime to d, X in [-10000, 10000], "
+            f"primes <= 2e9, merit > 22")
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (every 200 ms)."""
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+# ------------------------------------------------------------- CPU baseline
+
+def cpu_reference_estimate(threads: int, rows_per_thread: int = 1, seed: int = 1) -> dict:
+    """m/sec of the reference's CPU path on this host, from a bounded sample.
+
+    The path is the reference's sieve -- one row per X across every m of the
+    window, every prime <= max_prime (gap_search_gpu.cpp:586-689, corrected)
+    -- followed by GMP strong-PRP tests outward from X = 0 (the overflow path
+    of overflow.cpp:145-160 applied to both sides).  The sample: `threads`
+    X rows of the sieve (only X coprime to K's primes cost anything; the
+    rest are whole-row composites), scaled to all such rows; the PRP tests
+    per m measured by the oracle's search on `threads` sampled m; the time of
+    one GMP strong base-2 test measured on a batch of candidates of the
+    workload's size.
+    """
+    import random
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O  # the CPU restatement (the reference cannot be built in this image)
+    W = WORKLOAD
+    rng = random.Random(seed)
+    t0 = time.perf_counter()
+    job = O.Job(W["p"], W["d"], W["sl"], W["max_prime"], threads=threads)
+    setup_s = time.perf_counter() - t0
+    sly = W["sl"] // 2
+    kprimes = [q for q in range(3, W["p"] + 1, 2) if all(q % r for r in range(3, int(q ** 0.5) + 1, 2))
+               and W["d"] % q != 0]
+    real = [y for y in range(-sly, sly + 1) if y != 0 and all(y % q for q in kprimes)]
+    R = max(1, threads * rows_per_thread)
+    ys = [real[(i * len(real)) // R] for i in range(R)]
+    t1 = time.perf_counter()
+    job.sieve_x_rows(W["m_start"], W["m_inc"], ys)
+    t_rows = time.perf_counter() - t1
+    sieve_s = t_rows * len(real) / R
+    ms_all = O.coprime_ms(W["m_start"], W["m_inc"], W["d"])
+    sample_ms = sorted(rng.sample(list(ms_all), threads))
+    t2 = time.perf_counter()
+    _, _, _, tests = job.search(sample_ms, 1)
+    t_search = time.perf_counter() - t2
+    tests_per_m = tests / len(sample_ms)
+    cands = []
+    for _ in range(threads * 24):
+        m = int(rng.choice(ms_all))
+        cands.append(m * job.K + 2 * rng.randrange(-sly, sly) + 1 - 1)
+    cands = [c if c % 2 else c + 1 for c in cands]
+    t3 = time.perf_counter()
+    O.prp_batch(cands, 1, threads)
+    t_prp = time.perf_counter() - t3
+    per_test = t_prp * threads / len(cands)          # seconds of one core per test
+    prp_s = len(ms_all) * tests_per_m * per_test / threads
+    total = sieve_s + prp_s
+    job.close()
+    return {"value": len(ms_all) / total, "unit": "m/s", "cores": threads, "kind": "port",
+            "sample": (f"{R} of {len(real)} sieve rows (X coprime to K) over all {len(ms_all)} m, "
+                       f"scaled; PRP tests/m from the oracle search of {len(sample_ms)} m "
+                       f"({tests_per_m:.1f}/m); {len(cands)} GMP strong base-2 tests timed "
+                       f"({per_test * 1e6:.1f} us/test/core)"),
+            "sieve_seconds_full": sieve_s, "prp_seconds_full": prp_s,
+            "prp_tests_per_sec": len(ms_all) * tests_per_m / total,
+            "sample_seconds": t_rows + t_search + t_prp, "table_setup_seconds": setup_s}
+
+
+def host_threads() -> int:
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------- GPU arm
+
+def products_per_test(bits: int) -> int:
+    """Limb products of one test by the fixed formula 2*L^2*(B + ceil(B/w)), L = ceil(B/32)."""
+    L = (bits + 31) // 32
+    return 2 * L * L * (bits + (bits + WINDOW_BITS - 1) // WINDOW_BITS)
+
+
+def traffic_per_launch() -> dict | None:
+    f = ROOT / "profiles" / "ncu_traffic.json"
+    if f.exists():
+        try:
+            return json.loads(f.read_text())
+        except ValueError:
+            return None
+    return None
+
+
+def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
+    import torch
+    import __graft_entry__
+    pg = __graft_entry__.load_package()
+    torch.cuda.set_device(local_rank)
+    W = WORKLOAD
+    m_start = RANK_STARTS[rank]
+    m_inc = W["m_inc"]
+    ctx = pg.Context(local_rank)
+    t0 = time.perf_counter()
+    job = pg.Job(W["p"], W["d"], W["sl"], W["max_prime"], max_m_inc=m_inc, max_m=max(RANK_STARTS) + m_inc,
+                 rounds=1, ctx=ctx)
+    setup_s = time.perf_counter() - t0
+    imad_peak = ctx.imad_peak()
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", local_rank))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(form: int, steps: int, sampler: bool):
+        barrier()
+        clk = ClockSampler(local_rank) if sampler else None
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        stats = []
+        for _ in range(steps):
+            res = job.search(m_start, m_inc, form)
+            stats.append(res.stats)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        bracket_ms = ev0.elapsed_time(ev1)
+        clocks = clk.stop() if clk else None
+        barrier()
+        return res, stats, bracket_ms, clocks
+
+    for _ in range(args.warmup):
+        res = job.search(m_start, m_inc, pg.PG_SEARCH_PERSISTENT)
+    res, stats, bracket_ms, clocks = timed(pg.PG_SEARCH_PERSISTENT, args.steps, True)
+    dev_ms = sum(s["total_ms"] for s in stats)
+    kern_ms = sum(s["search_kernel_ms"] for s in stats)
+    tests = sum(s["prp_tests"] for s in stats)
+    m_count = stats[0]["m_count"]
+    # plain form, same window (the batched-vs-plain A/B)
+    plain = None
+    if not args.no_plain:
+        job.search(m_start, m_inc, pg.PG_SEARCH_PLAIN)
+        _, pstats, pbracket, _ = timed(pg.PG_SEARCH_PLAIN, args.steps, False)
+        pdev = sum(s["total_ms"] for s in pstats)
+        plain = {"ms_per_step": pdev / args.steps, "m_per_sec": m_count * args.steps / (pdev / 1e3),
+                 "prp_tests": pstats[0]["prp_tests"], "passes": pstats[0]["passes"],
+                 "kernel_launches_per_step": pstats[0]["kernel_launches"]}
+    # end to end through the public API: host window in, host gaps + records out
+    barrier()
+    t_e2e = time.perf_counter()
+    nrec = 0
+    for _ in range(args.steps):
+        r = job.search(m_start, m_inc, pg.PG_SEARCH_PERSISTENT)
+        nrec += len(job.records(r, W["min_merit"]))
+    e2e_s = time.perf_counter() - t_e2e
+    barrier()
+    # bit-exactness self-check of this run against the committed GMP fixture
+    exact = None
+    if rank == 0:
+        gold = json.loads((ROOT / "tests" / "golden" / "gaps_cfg2.json").read_text())
+        pos = {int(m): i for i, m in enumerate(res.ms)}
+        exact = all((int(res.prev_gap[pos[m]]), int(res.next_gap[pos[m]])) == (a, b)
+                    for m, a, b in zip(gold["ms"], gold["prev_gap"], gold["next_gap"]))
+    mine = {"dev_s": dev_ms / 1e3, "bracket_s": bracket_ms / 1e3, "kern_s": kern_ms / 1e3, "tests": tests,
+            "m": m_count * args.steps, "e2e_s": e2e_s, "clocks": clocks,
+            "launches": sum(s["kernel_launches"] for s in stats)}
+    allr = [mine]
+    if dist is not None:
+        allr = [None] * world
+        dist.all_gather_object(allr, mine)
+    if rank != 0:
+        return None
+    dev_s = max(r["dev_s"] for r in allr)
+    tot_m = sum(r["m"] for r in allr)
+    bits = (job.K * (m_start + m_inc // 2)).bit_length()
+    ppt = products_per_test(bits)
+    achieved = tests * ppt / (kern_ms / 1e3)           # rank 0's kernel, products/s
+    peak = imad_peak / 2                               # a 32x32->64 product needs a lo and a hi multiply-add
+    tr = traffic_per_launch()
+    roof = {"bound": "imad", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "G limb-products/s",
+            "frac": achieved / peak, "traffic": tr.get("bytes_per_launch") if tr else None,
+            "kernel": "k_search_persistent<22>",
+            "work": f"{ppt} limb products per {bits}-bit test (2*L^2*(B+ceil(B/5)), L=ceil(B/32)), "
+                    f"{tests // args.steps} tests per launch",
+            "peak_source": "in-run microbenchmark (pg_measure_imad_peak: 32-bit IMAD/s / 2); "
+                           "MEASURED_PEAKS.json has no integer-multiply figure"}
+    line = {
+        "metric": METRIC, "value": tot_m / dev_s, "unit": "m/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": workload_name(RANK_STARTS[0], m_inc), "form": "persistent",
+                   "m_per_gpu_per_step": m_count, "sl": W["sl"], "max_prime": W["max_prime"],
+                   "limbs": job.info["limbs"], "parallelism": f"weak: {world} disjoint m-windows",
+                   "l2": "inputs larger than L2 (786 MB prime tables read every step)"},
+        "prp_tests_per_sec": sum(r["tests"] for r in allr) / dev_s,
+        "ms_per_step_bracket": max(r["bracket_s"] for r in allr) * 1e3 / args.steps,
+        "setup_seconds": setup_s,
+        "bit_exact_vs_gmp_sample": exact,
+        "roofline": roof,
+        "e2e": {"value": tot_m / max(r["e2e_s"] for r in allr), "unit": "m/s",
+                "h2d_bytes_per_step": stats[0]["h2d_bytes"], "d2h_bytes_per_step": stats[0]["d2h_bytes"],
+                "records_per_step": nrec // max(1, args.steps)},
+        "gpu_launches": sum(r["launches"] for r in allr),
+        "clocks": allr[0]["clocks"],
+    }
+    if plain is not None:
+        line["plain"] = plain
+        line["batched_vs_plain"] = line["value"] / world / plain["m_per_sec"] if world == 1 else \
+            (tot_m / dev_s) / (plain["m_per_sec"] * world)
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_reference_estimate(host_threads())
+    job.close()
+    ctx.close()
+    return line
+
+
+def run_reference(args) -> dict:
+    threads = host_threads()
+    vals, last = [], None
+    for i in range(args.warmup + args.steps):
+        est = cpu_reference_estimate(threads, seed=i + 1)
+        if i >= args.warmup:
+            vals.append(est["value"])
+            last = est
+    v = statistics.median(vals)
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "m/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": workload_name(WORKLOAD["m_start"], WORKLOAD["m_inc"]),
+                       "implementation": "CPU restatement of the reference path (oracle/, GMP 6.3.0); "
+                                         "the reference needs CGBN and primesieve, absent here"},
+            "cpu_baseline": {**{k: last[k] for k in ("unit", "cores", "kind", "sample")}, "value": v},
+            "e2e": {"value": v, "unit": "m/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "prp_tests_per_sec": last["prp_tests_per_sec"]}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-form A/B")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    args = ap.parse_args(argv)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return 0
+    if world > len(RANK_STARTS):
+        raise SystemExit(f"at most {len(RANK_STARTS)} ranks")
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dd
+        torch.cuda.set_device(local_rank)
+        dd.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                              device_id=torch.device("cuda", local_rank))
+        dist = dd
+    try:
+        line = run_ours(args, rank, world, local_rank, dist)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

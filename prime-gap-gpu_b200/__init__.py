@@ -305,12 +305,16 @@ class Job:
 
     def records(self, res: SearchResult, min_merit: float) -> list[str]:
         """Record lines of every gap with merit > min_merit (overflow.cpp:162-188, strict >)."""
+        gaps = res.prev_gap.astype(np.float64) + res.next_gap.astype(np.float64)
+        approx = gaps / (self.k_log + np.log(res.ms.astype(np.float64)))
         out = []
-        for m, pg, ng in zip(res.ms, res.prev_gap, res.next_gap):
-            gap = int(pg) + int(ng)
-            mer = merit(self.k_log, int(m), gap)
+        # numpy's log may differ from libm's in the last ulp: pre-filter with a
+        # margin, then decide with the exact formula of overflow.cpp:162
+        for i in np.nonzero(approx > min_merit - 1e-6)[0]:
+            m, pg, ng = int(res.ms[i]), int(res.prev_gap[i]), int(res.next_gap[i])
+            mer = merit(self.k_log, m, pg + ng)
             if mer > min_merit:
-                out.append(format_record(gap, mer, int(m), self.p, self.d, int(pg)))
+                out.append(format_record(pg + ng, mer, m, self.p, self.d, pg))
         return out
 
 

@@ -21,6 +21,7 @@ PKG = pathlib.Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "build"
 LIB = BUILD / "libprimegap.so"
+CLI = BUILD / "gap_search_gpu"
 ROOT = PKG.parent
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -90,6 +91,16 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
             raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
         if verbose:
             print("linked", LIB, flush=True)
+    cli_src = CSRC / "gap_search_gpu.cpp"
+    if cli_src.exists() and (force or not CLI.exists() or CLI.stat().st_mtime < max(
+            LIB.stat().st_mtime, cli_src.stat().st_mtime)):
+        cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-Wall", f"-I{ROOT / 'include'}", str(cli_src),
+               "-o", str(CLI), f"-L{BUILD}", "-lprimegap", "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"CLI build failed:\n{r.stderr[-4000:]}")
+        if verbose:
+            print("built", CLI, flush=True)
     return LIB
 
 

@@ -1,0 +1,243 @@
+// gap_search_gpu -- command line of the prime-gap search on the B200 library.
+//
+// Keeps the reference's flags and output (gap_common.cpp:313-492,
+// gap_search_gpu.cpp:106-175, overflow.cpp:179-188):
+//   -p P -d D --mstart M --minc I --max-prime MILLIONS --min-merit F
+//   --cpu-fraction F --cpu-threads N   (accepted; there is no CPU finishing)
+//   --hide-timing --testing -q -v -h
+// and adds:
+//   --sl X        search radius: X in [-sl, sl] is sieved (default 8*ln(N), even)
+//   --ranges R    windows of --minc m to search; 0 = until Ctrl-C (the reference's only mode)
+//   --chunk C     m per device call (default min(minc, 1,000,000))
+//   --form persistent|plain   --rounds R   --device N
+// Record lines "{gap} {merit:.3f} {m} * {P}# / {D} - {prev}" go to stdout and
+// are appended to records_{P}.txt.  Ctrl-C once: finish the current window;
+// twice: stop after the current device call; three times: exit(2)
+// (gap_search_gpu.cpp:1050-1069).
+#include <getopt.h>
+
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <csignal>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/primegap.h"
+
+struct Config {
+    int valid = 1;
+    uint32_t p = 0, d = 0;
+    uint64_t m_start = 0, m_inc = 0;
+    float min_merit = 18;
+    uint64_t max_prime = 0;
+    float cpu_fraction = 0.005f;
+    int cpu_threads = 3;
+    int verbose = 1;
+    bool show_timing = true;
+    bool testing = false;
+    // additions
+    uint32_t sl = 0;
+    uint64_t ranges = 0;
+    uint64_t chunk = 0;
+    int form = PG_SEARCH_PERSISTENT;
+    uint32_t rounds = 1;
+    int device = 0;
+};
+
+static void show_usage(const char *name) {
+    printf("Usage: %s\n[REQUIRED]\n  -p <p>\n  -d <p>\n  --mstart <start>\n  --minc   <int>\n\n", name);
+    printf("[OPTIONALLY]\n  --min-merit <min_merit>\n    only display prime gaps with merit >= min_merit\n");
+    printf("  --max-prime\n    use primes <= max-prime (in millions) for checking composite\n\n");
+    printf("  --cpu-fraction <fraction>   (accepted for compatibility; no CPU finishing)\n");
+    printf("  --cpu-threads <n>           (accepted for compatibility; no CPU finishing)\n");
+    printf("  --sl <X>        sieve X in [-sl, sl] around m*K (default 8*ln(m*K))\n");
+    printf("  --ranges <R>    search R windows of minc m, 0 = until Ctrl-C (default 0)\n");
+    printf("  --chunk <C>     m per device call (default min(minc, 1000000))\n");
+    printf("  --form persistent|plain   --rounds <bases>   --device <n>\n\n");
+    printf("[OPTIONAL]\n  -q, --quiet\n  -v, --verbose\n  -h, --help\n");
+}
+
+static bool is_prime(uint64_t n) {
+    if (n < 2) return false;
+    for (uint64_t t = 2; t * t <= n; t++)
+        if (n % t == 0) return false;
+    return true;
+}
+
+static Config argparse(int argc, char **argv) {
+    static struct option long_options[] = {
+        {"p", required_argument, 0, 'p'},         {"d", required_argument, 0, 'd'},
+        {"mstart", required_argument, 0, 1},      {"minc", required_argument, 0, 2},
+        {"min-merit", required_argument, 0, 4},   {"max-prime", required_argument, 0, 5},
+        {"cpu-fraction", required_argument, 0, 7}, {"cpu-threads", required_argument, 0, 8},
+        {"hide-timing", no_argument, 0, 11},      {"testing", no_argument, 0, 12},
+        {"sl", required_argument, 0, 20},         {"ranges", required_argument, 0, 21},
+        {"chunk", required_argument, 0, 22},      {"form", required_argument, 0, 23},
+        {"rounds", required_argument, 0, 24},     {"device", required_argument, 0, 25},
+        {"quiet", no_argument, 0, 'q'},           {"verbose", no_argument, 0, 'v'},
+        {"help", no_argument, 0, 'h'},            {0, 0, 0, 0}};
+    Config c;
+    int idx = 0, ch;
+    while ((ch = getopt_long(argc, argv, "qvhp:d:", long_options, &idx)) >= 0) {
+        switch (ch) {
+            case 'h': show_usage(argv[0]); exit(0);
+            case 'q': c.verbose--; break;
+            case 'v': c.verbose++; break;
+            case 'p': c.p = (uint32_t)atoi(optarg); break;
+            case 'd': c.d = (uint32_t)atoi(optarg); break;
+            case 1: c.m_start = strtoull(optarg, nullptr, 10); break;
+            case 2: c.m_inc = strtoull(optarg, nullptr, 10); break;
+            case 4: c.min_merit = (float)atof(optarg); break;
+            case 5: c.max_prime = strtoull(optarg, nullptr, 10) * 1000000ull; break;
+            case 7: c.cpu_fraction = (float)atof(optarg); break;
+            case 8: c.cpu_threads = atoi(optarg); break;
+            case 11: c.show_timing = false; break;
+            case 12: c.testing = true; break;
+            case 20: c.sl = (uint32_t)strtoul(optarg, nullptr, 10); break;
+            case 21: c.ranges = strtoull(optarg, nullptr, 10); break;
+            case 22: c.chunk = strtoull(optarg, nullptr, 10); break;
+            case 23:
+                if (!strcmp(optarg, "persistent")) c.form = PG_SEARCH_PERSISTENT;
+                else if (!strcmp(optarg, "plain")) c.form = PG_SEARCH_PLAIN;
+                else c.valid = 0;
+                break;
+            case 24: c.rounds = (uint32_t)atoi(optarg); break;
+            case 25: c.device = atoi(optarg); break;
+            default: c.valid = 0;
+        }
+    }
+    if (optind < argc) {
+        c.valid = 0;
+        printf("unknown positional argument: ");
+        while (optind < argc) printf("%s ", argv[optind++]);
+        printf("\n");
+    }
+    // validation (gap_common.cpp:416-490; the m parity, 2e9 prime and BITS limits are lifted)
+    if (c.m_start == 0) { c.valid = 0; printf("mstart must be greater than 0\n"); }
+    if (c.m_inc == 0) { c.valid = 0; printf("m_inc must be greater than 0\n"); }
+    if (c.max_prime < 1000) { c.valid = 0; printf("max_prime must be set\n"); }
+    if (c.max_prime >= (1ull << 40)) { c.valid = 0; printf("max_prime must be below 2^40\n"); }
+    if (!is_prime(c.p) || c.p >= 10000000) { printf("p# not prime (p=%u)\n", c.p); exit(1); }
+    if (c.d == 0 || c.d % 2) { c.valid = 0; printf("d must be even and greater than 0: %u\n", c.d); }
+    if (c.cpu_fraction < .00001f || c.cpu_fraction > .1f) { c.valid = 0; printf("cpu-fraction must be between .00001 and .1\n"); }
+    if (c.cpu_threads < 1 || c.cpu_threads > 159) { c.valid = 0; printf("cpu-threads must be between 1 and 159\n"); }
+    if (c.rounds < 1 || c.rounds > 16) { c.valid = 0; printf("rounds must be in 1..16\n"); }
+    return c;
+}
+
+static std::atomic<int> g_stop{0};
+static void on_sigint(int) {
+    const int n = ++g_stop;
+    if (n == 1) printf("\nCaught CTRL+C stopping, winding down work.\n\n");
+    else if (n == 2) printf("\nCaught 2nd CTRL+C, stopping after the current device call\n");
+    else { printf("\nCaught 3nd CTRL+C, exit(2) now.\n"); exit(2); }
+}
+
+#define CHECK(call)                                                              \
+    do {                                                                         \
+        int rc_ = (call);                                                        \
+        if (rc_ != PG_OK) {                                                      \
+            fprintf(stderr, "ERROR %s: %s\n", #call, pg_last_error());           \
+            return 1;                                                            \
+        }                                                                        \
+    } while (0)
+
+int main(int argc, char **argv) {
+    Config c = argparse(argc, argv);
+    if (!c.valid) {
+        show_usage(argv[0]);
+        return 1;
+    }
+    if (c.verbose >= 0) printf("\nTesting m * %u#/%u\n", c.p, c.d);
+    const uint64_t chunk = c.chunk ? c.chunk : std::min<uint64_t>(c.m_inc, 1000000);
+    const uint64_t last_m = c.ranges ? c.m_start + c.ranges * c.m_inc : c.m_start + 1000 * c.m_inc;
+    pg_ctx *ctx = nullptr;
+    CHECK(pg_ctx_create(c.device, &ctx));
+    // default radius: 8 * ln(N), even (the serving configuration's SL)
+    uint32_t sl = c.sl;
+    pg_job_params prm{};
+    prm.p = c.p;
+    prm.d = c.d;
+    prm.max_prime = c.max_prime;
+    prm.max_m_inc = chunk;
+    prm.max_m = last_m;
+    prm.rounds = c.rounds;
+    if (!sl) {
+        // log(K) first from a throw-away job with a tiny radius
+        pg_job *probe = nullptr;
+        pg_job_params pp = prm;
+        pp.sl = 2;
+        pp.max_prime = std::min<uint64_t>(c.max_prime, 1000);
+        pp.max_m_inc = 2;
+        CHECK(pg_job_create(ctx, &pp, &probe));
+        pg_job_info pi{};
+        pg_job_get_info(probe, &pi);
+        pg_job_destroy(probe);
+        sl = 2 * (uint32_t)std::lround(4.0 * (pi.k_log + std::log((double)c.m_start)));
+    }
+    prm.sl = sl;
+    pg_job *job = nullptr;
+    CHECK(pg_job_create(ctx, &prm, &job));
+    pg_job_info info{};
+    pg_job_get_info(job, &info);
+    if (c.verbose >= 1) {
+        printf("K = %u bits, log(K) = %.2f\n", info.k_bits, info.k_log);
+        printf("sieve: %llu primes <= %llu, X in [-%u, %u], %u-word operands\n",
+               (unsigned long long)info.num_primes + info.num_small, (unsigned long long)c.max_prime, sl, sl,
+               info.limbs);
+        if (c.show_timing) printf("\tSetup took %.1f seconds\n", info.setup_seconds);
+        printf("Min Gap ~= %d (for merit > %.1f)\n", (int)(c.min_merit * (info.k_log + std::log((double)c.m_inc))),
+               c.min_merit);
+    }
+    std::signal(SIGINT, on_sigint);
+    char fname[64];
+    snprintf(fname, sizeof fname, "records_%u.txt", c.p);
+    FILE *rec = fopen(fname, "a");
+    std::vector<uint64_t> ms(chunk);
+    std::vector<uint32_t> prev(chunk), next(chunk);
+    uint64_t total_m = 0, total_tests = 0, total_primes = 0, total_ext = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    uint64_t m_start = c.m_start;
+    for (uint64_t r = 0; (c.ranges == 0 || r < c.ranges) && g_stop == 0; r++) {
+        for (uint64_t off = 0; off < c.m_inc && g_stop < 2; off += chunk) {
+            const uint64_t inc = std::min(chunk, c.m_inc - off);
+            pg_search_stats st{};
+            CHECK(pg_search(job, m_start + off, inc, c.form, ms.data(), prev.data(), next.data(), &st));
+            total_m += st.m_count;
+            total_tests += st.prp_tests;
+            total_primes += 2 * st.m_count;
+            total_ext += st.extended_sides;
+            for (uint64_t i = 0; i < st.m_count; i++) {
+                const uint64_t gap = (uint64_t)prev[i] + next[i];
+                const double merit = pg_merit(info.k_log, ms[i], gap);
+                if (merit > c.min_merit) {
+                    char line[160];
+                    pg_format_record(line, sizeof line, gap, merit, ms[i], c.p, c.d, prev[i]);
+                    printf("%s\n", line);
+                    if (rec) {
+                        fprintf(rec, "%s\n", line);
+                        fflush(rec);
+                    }
+                }
+            }
+        }
+        m_start += c.m_inc;
+        if (c.verbose >= 1) {
+            const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            printf("\nGPU Timings (%.0f seconds):\n", c.show_timing ? secs : 0.0);
+            printf("\tm               : %llu (%.0f/sec)\n", (unsigned long long)total_m, total_m / secs);
+            printf("\ttotal tests     : %llu (%.1f%% prime) (%.0f/sec)\n", (unsigned long long)total_tests,
+                   total_tests ? 100.0 * total_primes / total_tests : 0.0, total_tests / secs);
+            printf("\tpast sl         : %llu sides (continued on the device)\n\n", (unsigned long long)total_ext);
+        }
+    }
+    if (rec) fclose(rec);
+    pg_job_destroy(job);
+    pg_ctx_destroy(ctx);
+    return 0;
+}

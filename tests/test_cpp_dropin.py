@@ -1,0 +1,59 @@
+"""The C++ drop-in header (include/primegap_runner.hpp) compiles against the
+reference's call shape, links libprimegap.so, and (on a GPU) gives the
+reference's results."""
+from __future__ import annotations
+
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+GMP_SO = "/lib/x86_64-linux-gnu/libgmp.so.10"
+
+
+def build_dropin(pg, tmp_path):
+    exe = tmp_path / "runner_dropin"
+    lib_dir = pg.LIB_PATH.parent
+    cmd = ["g++", "-O1", "-std=c++17", "-Wall", f"-I{ROOT / 'include'}", f"-I{ROOT / 'tests' / 'cpp' / 'shim'}",
+           str(ROOT / "tests" / "cpp" / "runner_dropin.cpp"), "-o", str(exe), f"-L{lib_dir}", "-lprimegap",
+           GMP_SO, f"-Wl,-rpath,{lib_dir}"]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return exe
+
+
+def test_dropin_compiles_and_links(pg, tmp_path):
+    assert build_dropin(pg, tmp_path).exists()
+
+
+def test_cli_help(pg):
+    cli = pg.LIB_PATH.parent / "gap_search_gpu"
+    out = subprocess.run([str(cli), "-h"], capture_output=True, text=True)
+    assert out.returncode == 0
+    for flag in ("-p", "-d", "--mstart", "--minc", "--min-merit", "--max-prime", "--cpu-fraction", "--sl"):
+        assert flag in out.stdout
+
+
+@pytest.mark.gpu
+def test_dropin_results(pg, tmp_path):
+    exe = build_dropin(pg, tmp_path)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    res = dict(zip(map(int, out[0::2]), map(int, out[1::2])))
+    # 2^521-1 prime, 2^521+1 composite, 2047 passes base 2, 101 prime, 2^127-1 prime, past `active`: 0
+    assert res == {0: 1, 1: 0, 2: 1, 3: 1, 4: 1, 5: 0}
+
+
+@pytest.mark.gpu
+def test_cli_records(pg, tmp_path):
+    """gap_search_gpu on the P=337 window prints the GMP records of merit > 5."""
+    from conftest import golden
+    g = golden("gaps_cfg1.json")
+    cli = pg.LIB_PATH.parent / "gap_search_gpu"
+    out = subprocess.run([str(cli), "-p", "337", "-d", "2310", "--mstart", "10000000", "--minc", "10000",
+                          "--max-prime", "100", "--min-merit", "5", "--sl", "7500", "--ranges", "1", "-q"],
+                         capture_output=True, text=True, cwd=tmp_path, check=True).stdout
+    import re
+    rec = re.compile(r"^\d+ \d+\.\d{3} \d+ \* \d+# / \d+ - \d+$")
+    lines = [line for line in out.splitlines() if rec.match(line)]
+    assert lines == g["records"]
+    assert (tmp_path / "records_337.txt").read_text().splitlines() == g["records"]
