@@ -168,6 +168,36 @@ typedef struct {
 int pg_search(pg_job *job, uint64_t m_start, uint64_t m_inc, int form,
               uint64_t *ms, uint32_t *prev_gap, uint32_t *next_gap, pg_search_stats *stats);
 
+/* ------------------------------------------------------ allocation-free */
+
+/* Largest batch of pg_next_prime_noalloc. */
+#define PG_NOALLOC_MAX_N 65536
+
+/* Next probable prime without allocating device memory.  No counterpart in
+ * the reference.  It is for callers that cannot call cudaMalloc: code whose
+ * device memory is owned by another allocator (a framework's caching pool, a
+ * budget fixed at start-up) and code that must not stall a running pipeline
+ * on an allocation, which can synchronise the device.
+ *
+ * For each of the n numbers at d_numbers (n rows of `words` LE uint32, device
+ * memory) writes to d_steps[i] the smallest k < max_steps such that
+ * d_numbers[i] + 2k passes the strong base-2 test, or 0xFFFFFFFF if none
+ * does (even numbers and numbers below 3 give 0xFFFFFFFF).  Enqueued on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream) of the current
+ * device; returns without waiting.
+ *
+ * Its only working memory is a file-scope device array of
+ * PG_NOALLOC_MAX_N + 64 uint32 (257 KB), which every GPU that loads the
+ * library holds until the process exits.  The first call on each device
+ * looks up that array's device address (cudaGetSymbolAddress) with the
+ * device current: make the first call on a device before any stream capture.
+ * n above PG_NOALLOC_MAX_N is rejected (PG_ERR_ARG), words above 48
+ * (PG_ERR_UNSUPPORTED).  Every call shares the array and clears it before
+ * use, so calls that can overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller. */
+int pg_next_prime_noalloc(const uint32_t *d_numbers, uint32_t n, uint32_t words, uint32_t max_steps,
+                          uint32_t *d_steps, void *stream);
+
 /* Merit of a gap as overflow.cpp:162: gap / (k_log + log(m)). */
 double pg_merit(double k_log, uint64_t m, uint64_t gap);
 

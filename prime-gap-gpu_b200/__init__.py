@@ -45,7 +45,7 @@ EXPORTS = (
     "pg_ctx_create", "pg_ctx_destroy", "pg_ctx_stream", "pg_last_error", "pg_version", "pg_measure_imad_peak",
     "pg_prp_batch", "pg_prp_batch_device",
     "pg_job_create", "pg_job_destroy", "pg_job_get_info", "pg_job_k_words",
-    "pg_count_m", "pg_sieve_interval", "pg_search", "pg_merit", "pg_format_record",
+    "pg_count_m", "pg_sieve_interval", "pg_search", "pg_merit", "pg_format_record", "pg_next_prime_noalloc",
 )
 
 

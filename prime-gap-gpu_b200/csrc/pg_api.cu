@@ -44,6 +44,8 @@ static int fail(int code, const char *fmt, ...) {
     } while (0)
 
 extern "C" const char *pg_last_error(void) { return g_last_error.c_str(); }
+
+void pg::set_error(const char *msg) { g_last_error = msg; }
 extern "C" const char *pg_version(void) { return "primegap-b200 0.1 (sm_100a)"; }
 
 // ======================================================= host bignum (K)

@@ -95,6 +95,8 @@ cudaError_t launch_finalize(uint32_t L, const SearchArgs &a, uint32_t nsides, ui
                             uint32_t *k_start_rw, cudaStream_t st);
 cudaError_t launch_iota(uint32_t *out, uint32_t n, cudaStream_t st);
 cudaError_t launch_imad_peak(int grid, uint32_t iters, uint32_t *sink, cudaStream_t st);
+// records the calling thread's pg_last_error() text (pg_api.cu)
+void set_error(const char *msg);
 int search_grid(uint32_t L, int device);
 bool supported_limbs(uint32_t L);
 uint32_t pick_limbs(uint32_t words);  // smallest compiled L >= words, 0 if none

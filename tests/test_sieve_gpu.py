@@ -29,7 +29,7 @@ def test_golden_rows(pg):
     (503, 2190, 10_000, 20_000_000, 1_000_000, 3_000, 1_000),    # most primes in the large kernel
     (337, 2310, 7_500, 60_000, 10_000_000, 4_000, 0),            # limit below the small split
     (907, 210, 18_000, 5_000_000, 1_000_000, 1_000, 4_096),
-    (1201, 2190, 40_000, 3_000_000, 1, 600, 0),                  # m from 1, SL 40000, 1 193-bit K
+    (907, 2190, 40_000, 3_000_000, 1, 600, 0),                   # m from 1, SL 40000, 1 244-bit K
     (151, 2310, 1_234, 1_000_000, 956_702_000_001, 5_000, 0),    # odd m_start, m above 2^32
     (337, 2310, 3, 100_000, 10_000_000, 500, 0),                 # SL = 3: one position per side
 ])
