@@ -164,6 +164,9 @@ struct pg_job {
     void *d_lp = nullptr, *d_lc = nullptr, *d_lcinv = nullptr;
     uint64_t np = 0;
     bool wide = false;
+    // prime table index of each sieve segment (segment s starts at value seg_v0 + s * seg_span)
+    std::vector<uint64_t> seg_off;
+    uint64_t seg_v0 = 0, seg_span = 0;
     // window buffers
     uint64_t nm_cap = 0, nodd_cap = 0;
     uint64_t *d_ms = nullptr;
@@ -440,6 +443,9 @@ static int job_build(pg_job *j) {
             acc += cnt[i];
         }
         j->np = acc;
+        j->seg_off = off;
+        j->seg_v0 = v_first;
+        j->seg_span = seg_span;
         const size_t esz = j->wide ? 8 : 4;
         void *lp = nullptr, *lc = nullptr, *lci = nullptr;
         cudaError_t e1 = cudaMalloc(&lp, std::max<uint64_t>(acc, 1) * esz);
@@ -572,6 +578,22 @@ static int window_setup(pg_job *j, uint64_t m_start, uint64_t m_inc, uint64_t *m
     return PG_OK;
 }
 
+// First prime-table index sieved by modular search rather than by stepping
+// every Y: primes whose expected hits in the window, nodd * (2 sly + 1) / p,
+// fall below LARGE_SEARCH_HITS (the two methods cost about the same there).
+static constexpr double LARGE_SEARCH_HITS = 16.0;
+
+static uint64_t large_split(const pg_job *j, uint64_t nodd) {
+    if (j->np == 0) return 0;
+    if (j->prm.flags & PG_JOB_LARGE_STEP) return j->np;
+    if (j->prm.flags & PG_JOB_LARGE_SEARCH) return 0;
+    const double pv = (double)nodd * (2.0 * j->sly + 1) / LARGE_SEARCH_HITS;
+    if (pv <= (double)j->seg_v0) return 0;
+    const double s = (pv - (double)j->seg_v0) / (double)j->seg_span;
+    if (s >= (double)j->seg_off.size()) return j->np;
+    return j->seg_off[(size_t)s];
+}
+
 static int run_sieve(pg_job *j, uint64_t m0, uint64_t nodd, uint32_t nm, bool compact) {
     cudaStream_t st = j->ctx->stream;
     PG_CUDA(cudaMemsetAsync(j->d_bitmaps, 0, (size_t)nm * j->W * 4, st));
@@ -587,7 +609,7 @@ static int run_sieve(pg_job *j, uint64_t m0, uint64_t nodd, uint32_t nm, bool co
     la.p = j->d_lp;
     la.cinv = j->d_lcinv;
     la.c = j->d_lc;
-    PG_CUDA(launch_sieve_large(la, j->wide, 0, st));
+    PG_CUDA(launch_sieve_large(la, j->wide, large_split(j, nodd), st));
     SieveArgs sa{};
     sa.sly = j->sly;
     sa.words = j->W;

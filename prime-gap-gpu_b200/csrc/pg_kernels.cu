@@ -242,15 +242,142 @@ __global__ void __launch_bounds__(256) k_sieve_large_step(const __grid_constant_
     }
 }
 
-cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, int method, cudaStream_t st) {
-    (void)method;
+// ------------------------------------------------- modular search, 32-bit p
+
+// Smallest x >= 0 with (A*x + B) mod M <= W, for 0 < A < M, B < M, W < M,
+// gcd(A, M) = 1.  If B <= W, x = 0.  If W+1 >= A the first wrap (y = 1)
+// already lands in the window: x = ceil((M-B)/A).  Otherwise the first
+// wrap count y >= 1 whose interval [M*y - B, M*y - B + W] holds a multiple
+// of A solves, after the reflection z -> W - z, the same problem for
+// (M mod A, ., A, W): a Euclid step, so the depth is O(log M).  The
+// levels are kept on a small stack and x = ceil((M*y - B)/A) is rebuilt on
+// the way back.
+__device__ __forceinline__ uint32_t modsearch32(uint32_t A, uint32_t B, uint32_t M, uint32_t W) {
+    uint32_t sA[48], sB[48], sM[48];
+    int lv = 0;
+    uint64_t x;
+    while (true) {
+        if (B <= W) {
+            x = 0;
+            break;
+        }
+        if (W + 1 >= A || lv == 48) {
+            x = (uint64_t)(M - B + A - 1) / A;
+            break;
+        }
+        sA[lv] = A;
+        sB[lv] = B;
+        sM[lv] = M;
+        lv++;
+        const uint32_t r = M % A;
+        uint32_t b1 = B % A;
+        b1 = b1 >= r ? b1 - r : b1 + (A - r);      // (B - M) mod A
+        const uint32_t b2 = W >= b1 ? W - b1 : W + (A - b1);  // reflected
+        M = A;
+        A = r;
+        B = b2;
+    }
+    while (lv > 0) {
+        lv--;
+        const uint64_t y = x + 1;
+        x = ((uint64_t)sM[lv] * y - sB[lv] + sA[lv] - 1) / sA[lv];
+    }
+    return (uint32_t)x;
+}
+
+// Same for 64-bit moduli (primes above 2^32): products need 128 bits.
+__device__ __forceinline__ uint64_t modsearch64(uint64_t A, uint64_t B, uint64_t M, uint64_t W) {
+    uint64_t sA[64], sB[64], sM[64];
+    int lv = 0;
+    unsigned __int128 x;
+    while (true) {
+        if (B <= W) {
+            x = 0;
+            break;
+        }
+        if (W + 1 >= A || lv == 64) {
+            x = (M - B + A - 1) / A;
+            break;
+        }
+        sA[lv] = A;
+        sB[lv] = B;
+        sM[lv] = M;
+        lv++;
+        const uint64_t r = M % A;
+        uint64_t b1 = B % A;
+        b1 = b1 >= r ? b1 - r : b1 + (A - r);
+        const uint64_t b2 = W >= b1 ? W - b1 : W + (A - b1);
+        M = A;
+        A = r;
+        B = b2;
+    }
+    while (lv > 0) {
+        lv--;
+        const unsigned __int128 y = x + 1;
+        x = ((unsigned __int128)sM[lv] * y - sB[lv] + sA[lv] - 1) / sA[lv];
+    }
+    return (uint64_t)x;
+}
+
+// One thread per prime p of [first, first + count).  With X = 2Y and the
+// odd m = m0 + 2j, p | m*K + X  <=>  u = Y + sly = (A*j + B) mod p with
+// A = -K mod p and B = sly - m0*K/2 mod p; every j of the window with
+// u <= 2*sly is a hit.  The next hit is found directly by modsearch, so a
+// prime costs O(log p) per hit instead of one step per Y.
+template <typename T>
+__global__ void __launch_bounds__(256) k_sieve_large_search(const __grid_constant__ LargeArgs a, uint64_t first,
+                                                            uint64_t count) {
+    const uint64_t i = first + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= first + count) return;
+    const uint64_t p = ((const T *)a.p)[i];
+    const uint64_t c = ((const T *)a.c)[i];
+    const uint64_t W = 2ull * a.sly;
+    const uint64_t inv2 = (p + 1) >> 1;
+    const uint64_t t = mulmod40(mulmod40(a.m0 % p, c, p), inv2, p);
+    const uint64_t sp = a.sly % p;
+    uint64_t B = sp >= t ? sp - t : sp + (p - t);
+    const uint64_t A = p - c;  // c in [1, p)
+    uint64_t j = 0;
+    while (j < a.nodd) {
+        uint64_t d, u;
+        if (p < (1ull << 32)) {
+            d = modsearch32((uint32_t)A, (uint32_t)B, (uint32_t)p, (uint32_t)W);
+            u = (A * d + B) % p;
+        } else {
+            d = modsearch64(A, B, p, W);
+            u = (uint64_t)(((unsigned __int128)A * d + B) % p);
+        }
+        j += d;
+        if (j >= a.nodd) break;
+        for (uint64_t uu = u; uu <= W; uu += p) mark_hit(a, j, (uint32_t)uu);
+        B = u + A >= p ? u + A - p : u + A;  // residue of j + 1
+        j++;
+    }
+}
+
+cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, cudaStream_t st) {
     if (a.np == 0) return cudaSuccess;
     const uint32_t threads = 256;
-    const uint64_t blocks = (a.np + threads - 1) / threads;
-    if (wide)
-        k_sieve_large_step<uint64_t><<<(unsigned)blocks, threads, 0, st>>>(a);
-    else
-        k_sieve_large_step<uint32_t><<<(unsigned)blocks, threads, 0, st>>>(a);
+    if (split > a.np) split = a.np;
+    if (split > 0) {  // primes with many hits per window: step every Y
+        LargeArgs s = a;
+        s.np = split;
+        const uint64_t blocks = (split + threads - 1) / threads;
+        if (wide)
+            k_sieve_large_step<uint64_t><<<(unsigned)blocks, threads, 0, st>>>(s);
+        else
+            k_sieve_large_step<uint32_t><<<(unsigned)blocks, threads, 0, st>>>(s);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (split < a.np) {  // the rest: modular search for each hit
+        const uint64_t count = a.np - split;
+        const uint64_t blocks = (count + threads - 1) / threads;
+        if (wide)
+            k_sieve_large_search<uint64_t><<<(unsigned)blocks, threads, 0, st>>>(a, split, count);
+        else
+            k_sieve_large_search<uint32_t><<<(unsigned)blocks, threads, 0, st>>>(a, split, count);
+    }
     return cudaGetLastError();
 }
 

@@ -42,6 +42,20 @@ def test_rows_match_oracle(pg, oracle, P, d, sl, limit, m_start, m_inc, small):
     assert np.array_equal(rows, want)
 
 
+@pytest.mark.parametrize("flags", [0, 1, 2])  # automatic split, step every Y, modular search
+@pytest.mark.parametrize("P,d,sl,limit,m_start,m_inc", [
+    (503, 2190, 10_000, 30_000_000, 1_000_000, 4_000),
+    (337, 2310, 200_000 // 2, 5_000_000, 10_000_000, 1_000),   # sly = 50 000 < small split: two hits per j
+    (907, 210, 2_000, 40_000_000, 1_000_000, 20_000),
+])
+def test_large_prime_methods_agree(pg, oracle, flags, P, d, sl, limit, m_start, m_inc):
+    with _job(pg, P, d, sl, limit, m_start, m_inc, flags=flags, small_limit=2_000) as job:
+        ms, rows = job.sieve_interval(m_start, m_inc)
+    with oracle.Job(P, d, sl, limit) as oj:
+        want = oj.sieve_m(ms)
+    assert np.array_equal(rows, want)
+
+
 def test_wide_primes_above_2_32(pg, oracle):
     """max_prime above 2^32: 64-bit prime tables and residues."""
     P, d, sl, limit, m_start, m_inc = 503, 2190, 4_000, 4_300_000_000, 1_000_000, 60
