@@ -107,6 +107,8 @@ typedef struct {
                               0 = default (65536) */
     uint32_t ext_window;   /* extension positions past sl tried in the first pass; 0 = 64 */
     uint32_t flags;        /* PG_JOB_* */
+    uint32_t search_hits;  /* large primes expecting fewer hits per window than this are sieved
+                              by modular search, the others by stepping every X; 0 = 16 */
 } pg_job_params;
 
 /* large-prime sieve: 0 = automatic, else force one method */
@@ -197,6 +199,26 @@ int pg_search(pg_job *job, uint64_t m_start, uint64_t m_inc, int form,
  * threads) race and must be serialised by the caller. */
 int pg_next_prime_noalloc(const uint32_t *d_numbers, uint32_t n, uint32_t words, uint32_t max_steps,
                           uint32_t *d_steps, void *stream);
+
+/* Pipelined search: a job has PG_SEARCH_SLOTS window slots (own stream and
+ * buffers each), so PG_SEARCH_SLOTS windows can be in flight and overlap on
+ * the device -- the reference keeps GPU_BATCHES batches in flight
+ * (gpu_testing.cu:57) for the same reason.  pg_search_submit enqueues the
+ * search of one window and returns a ticket (tickets count up from 0; ticket
+ * t uses slot t % PG_SEARCH_SLOTS, which must not hold an un-waited ticket,
+ * else PG_ERR_STATE).  pg_search_wait(ticket) blocks until that window is
+ * done and fills the outputs like pg_search.  flags: PG_SUBMIT_DRAIN lets
+ * the PRP kernel's warps leave once few sides remain unresolved, handing
+ * their SMs to the next window (for callers that keep another window
+ * submitted; a lone window finishes later with it).  pg_search() is
+ * submit + wait. */
+#define PG_SEARCH_SLOTS 2
+#define PG_SUBMIT_DRAIN 0x1u
+int pg_search_submit(pg_job *job, uint64_t m_start, uint64_t m_inc, int form, uint32_t flags, uint64_t *ticket);
+int pg_search_wait(pg_job *job, uint64_t ticket, uint64_t *ms, uint32_t *prev_gap, uint32_t *next_gap,
+                   pg_search_stats *stats);
+/* cudaStream_t of window slot `slot` (for CUDA-event timing by callers). */
+void *pg_job_stream(pg_job *job, int slot);
 
 /* Merit of a gap as overflow.cpp:162: gap / (k_log + log(m)). */
 double pg_merit(double k_log, uint64_t m, uint64_t gap);

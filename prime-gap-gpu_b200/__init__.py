@@ -46,7 +46,10 @@ EXPORTS = (
     "pg_prp_batch", "pg_prp_batch_device",
     "pg_job_create", "pg_job_destroy", "pg_job_get_info", "pg_job_k_words",
     "pg_count_m", "pg_sieve_interval", "pg_search", "pg_merit", "pg_format_record", "pg_next_prime_noalloc",
+    "pg_search_submit", "pg_search_wait", "pg_job_stream",
 )
+PG_SEARCH_SLOTS = 2
+PG_SUBMIT_DRAIN = 0x1
 
 
 class PrimeGapError(RuntimeError):
@@ -60,7 +63,7 @@ class JobParams(ctypes.Structure):
         ("p", ctypes.c_uint32), ("d", ctypes.c_uint32), ("sl", ctypes.c_uint32),
         ("max_prime", ctypes.c_uint64), ("max_m_inc", ctypes.c_uint64), ("max_m", ctypes.c_uint64),
         ("rounds", ctypes.c_uint32), ("small_limit", ctypes.c_uint32),
-        ("ext_window", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+        ("ext_window", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("search_hits", ctypes.c_uint32),
     ]
 
 
@@ -112,6 +115,10 @@ def _load() -> ctypes.CDLL:
     lib.pg_count_m.argtypes = [u64, u64, u32]
     lib.pg_sieve_interval.argtypes = [vp, u64, u64, P64, P32]
     lib.pg_search.argtypes = [vp, u64, u64, i32, P64, P32, P32, ctypes.POINTER(SearchStats)]
+    lib.pg_search_submit.argtypes = [vp, u64, u64, i32, u32, ctypes.POINTER(ctypes.c_uint64)]
+    lib.pg_search_wait.argtypes = [vp, u64, P64, P32, P32, ctypes.POINTER(SearchStats)]
+    lib.pg_job_stream.restype = vp
+    lib.pg_job_stream.argtypes = [vp, i32]
     lib.pg_merit.restype = ctypes.c_double
     lib.pg_merit.argtypes = [ctypes.c_double, u64, u64]
     lib.pg_format_record.argtypes = [ctypes.c_char_p, ctypes.c_size_t, u64, ctypes.c_double, u64, u32, u32, u64]
@@ -246,9 +253,10 @@ class Job:
 
     def __init__(self, p: int, d: int, sl: int, max_prime: int, max_m_inc: int, max_m: int,
                  rounds: int = 1, small_limit: int = 0, ext_window: int = 0, flags: int = 0,
-                 ctx: Context | None = None, device: int = 0):
+                 search_hits: int = 0, ctx: Context | None = None, device: int = 0):
         self.ctx = ctx or Context(device)
-        self.params = JobParams(p, d, sl, max_prime, max_m_inc, max_m, rounds, small_limit, ext_window, flags)
+        self.params = JobParams(p, d, sl, max_prime, max_m_inc, max_m, rounds, small_limit, ext_window, flags,
+                                search_hits)
         h = ctypes.c_void_p()
         _check(lib.pg_job_create(self.ctx.handle, ctypes.byref(self.params), ctypes.byref(h)))
         self._h = h
@@ -298,6 +306,29 @@ class Job:
         st = SearchStats()
         _check(lib.pg_search(self._h, m_start, m_inc, form, _p64(ms), _p32(prev), _p32(nxt), ctypes.byref(st)))
         return SearchResult(ms, prev, nxt, st.as_dict())
+
+    def submit(self, m_start: int, m_inc: int, form: int = PG_SEARCH_PERSISTENT, flags: int = 0) -> int:
+        """Enqueue the search of a window; returns a ticket for wait().  Up to
+        PG_SEARCH_SLOTS windows may be in flight (they overlap on the device)."""
+        t = ctypes.c_uint64(0)
+        _check(lib.pg_search_submit(self._h, m_start, m_inc, form, flags, ctypes.byref(t)))
+        if not hasattr(self, "_pending"):
+            self._pending = {}
+        self._pending[t.value] = count_m(m_start, m_inc, self.d)
+        return t.value
+
+    def wait(self, ticket: int) -> SearchResult:
+        n = self._pending.pop(ticket)
+        ms = np.zeros(n, dtype=np.uint64)
+        prev = np.zeros(n, dtype=np.uint32)
+        nxt = np.zeros(n, dtype=np.uint32)
+        st = SearchStats()
+        _check(lib.pg_search_wait(self._h, ticket, _p64(ms), _p32(prev), _p32(nxt), ctypes.byref(st)))
+        return SearchResult(ms, prev, nxt, st.as_dict())
+
+    def stream_ptr(self, slot: int) -> int:
+        """cudaStream_t of a window slot (for CUDA-event timing)."""
+        return int(lib.pg_job_stream(self._h, slot) or 0)
 
     def merits(self, res: SearchResult) -> np.ndarray:
         return np.array([merit(self.k_log, int(m), int(a) + int(b))

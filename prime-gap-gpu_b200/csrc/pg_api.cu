@@ -3,11 +3,13 @@
 // Job set-up builds K = P#/d with a small host bignum (gap_common.cpp:60-65),
 // the K-prime wheel and the small-prime tables on the host, and the large
 // prime table (every prime in (small_limit, max_prime] with K mod p and
-// K^-1 mod p) on the device.  pg_search runs, on the context's stream,
-//   memset -> large-prime sieve -> small-prime sieve + survivor lists ->
-//   PRP search (persistent or plain) -> finalize/confirm -> continuation,
-// and copies the gaps back.  No function exits the process; errors come back
-// as PG_ERR_* with a message in pg_last_error().
+// K^-1 mod p) on the device.  A job has PG_SEARCH_SLOTS window slots, each
+// with its own stream and buffers, so consecutive windows overlap on the
+// device.  A search of one window runs on its slot's stream:
+//   large-prime sieve -> small-prime sieve + survivor lists -> PRP search
+//   (persistent or plain) -> finalize/confirm [-> continuation launches]
+// No function exits the process; errors come back as PG_ERR_* with a message
+// in pg_last_error().
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -46,7 +48,8 @@ static int fail(int code, const char *fmt, ...) {
 extern "C" const char *pg_last_error(void) { return g_last_error.c_str(); }
 
 void pg::set_error(const char *msg) { g_last_error = msg; }
-extern "C" const char *pg_version(void) { return "primegap-b200 0.1 (sm_100a)"; }
+
+extern "C" const char *pg_version(void) { return "primegap-b200 0.2 (sm_100a)"; }
 
 // ======================================================= host bignum (K)
 
@@ -138,14 +141,28 @@ struct pg_ctx {
     size_t cand_cap = 0, res_cap = 0;
 };
 
-struct Scalars {  // device scalars of one window
-    unsigned long long next_item;
-    unsigned long long tests;
-    unsigned long long confirm;
-    uint32_t n_redo;
-    uint32_t n_out;
-    uint32_t max_count;
-    uint32_t pad;
+// One window in flight: its buffers, stream, events and the host state
+// needed to finish it.
+struct WinSlot {
+    cudaStream_t st = nullptr;
+    uint64_t *d_ms = nullptr;
+    int32_t *d_rank = nullptr;
+    uint32_t *d_bitmaps = nullptr;
+    uint16_t *d_lists = nullptr;
+    uint32_t *d_counts = nullptr, *d_found = nullptr, *d_kstart = nullptr, *d_knext = nullptr, *d_gaps = nullptr;
+    uint32_t *d_act0 = nullptr, *d_act1 = nullptr, *d_redo = nullptr;
+    Scalars *d_sc = nullptr;
+    Scalars *h_sc = nullptr;    // pinned
+    uint64_t *h_ms = nullptr;   // pinned
+    int32_t *h_rank = nullptr;  // pinned
+    uint32_t *h_gaps = nullptr; // pinned
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    // in-flight state
+    bool busy = false;
+    uint64_t ticket = 0;
+    uint64_t m0 = 0, nodd = 0;
+    uint32_t nm = 0;
+    pg_search_stats sst{};
 };
 
 struct pg_job {
@@ -167,19 +184,10 @@ struct pg_job {
     // prime table index of each sieve segment (segment s starts at value seg_v0 + s * seg_span)
     std::vector<uint64_t> seg_off;
     uint64_t seg_v0 = 0, seg_span = 0;
-    // window buffers
+    // window slots
     uint64_t nm_cap = 0, nodd_cap = 0;
-    uint64_t *d_ms = nullptr;
-    int32_t *d_rank = nullptr;
-    uint32_t *d_bitmaps = nullptr;
-    uint16_t *d_lists = nullptr;
-    uint32_t *d_counts = nullptr, *d_found = nullptr, *d_kstart = nullptr, *d_knext = nullptr, *d_gaps = nullptr;
-    uint32_t *d_act0 = nullptr, *d_act1 = nullptr, *d_redo = nullptr;
-    Scalars *d_sc = nullptr;
-    Scalars *h_sc = nullptr;  // pinned
-    uint64_t *h_ms = nullptr;  // pinned
-    int32_t *h_rank = nullptr; // pinned
-    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    WinSlot slot[PG_SEARCH_SLOTS];
+    uint64_t next_ticket = 0;
     uint64_t dev_bytes = 0;
     int grid = 0;
 };
@@ -313,20 +321,27 @@ extern "C" uint64_t pg_count_m(uint64_t m_start, uint64_t m_inc, uint32_t d) {
     return c;
 }
 
+static void slot_free(WinSlot &s) {
+    if (s.st) cudaStreamSynchronize(s.st);
+    void *ptrs[] = {s.d_ms,   s.d_rank,   s.d_bitmaps, s.d_lists, s.d_counts, s.d_found, s.d_kstart,
+                    s.d_knext, s.d_gaps,  s.d_act0,    s.d_act1,  s.d_redo,   s.d_sc};
+    for (void *p : ptrs) cudaFree(p);
+    cudaFreeHost(s.h_sc);
+    cudaFreeHost(s.h_ms);
+    cudaFreeHost(s.h_rank);
+    cudaFreeHost(s.h_gaps);
+    for (auto &e : s.ev)
+        if (e) cudaEventDestroy(e);
+    if (s.st) cudaStreamDestroy(s.st);
+}
+
 static void job_free(pg_job *j) {
     if (!j) return;
     cudaSetDevice(j->ctx->device);
     cudaStreamSynchronize(j->ctx->stream);
-    void *ptrs[] = {j->d_wheel, j->d_sq,   j->d_sr,     j->d_sbar,  j->d_tq,     j->d_tr,    j->d_lp,
-                    j->d_lc,    j->d_lcinv, j->d_ms,    j->d_rank,  j->d_bitmaps, j->d_lists, j->d_counts,
-                    j->d_found, j->d_kstart, j->d_knext, j->d_gaps, j->d_act0,   j->d_act1,  j->d_redo,
-                    j->d_sc};
+    for (auto &s : j->slot) slot_free(s);
+    void *ptrs[] = {j->d_wheel, j->d_sq, j->d_sr, j->d_sbar, j->d_tq, j->d_tr, j->d_lp, j->d_lc, j->d_lcinv};
     for (void *p : ptrs) cudaFree(p);
-    cudaFreeHost(j->h_sc);
-    cudaFreeHost(j->h_ms);
-    cudaFreeHost(j->h_rank);
-    for (auto &e : j->ev)
-        if (e) cudaEventDestroy(e);
     delete j;
 }
 
@@ -336,6 +351,24 @@ extern "C" int pg_job_destroy(pg_job *j) {
 }
 
 static uint32_t bitlen64(uint64_t v) { return v ? 64 - __builtin_clzll(v) : 0; }
+
+static int slot_alloc(pg_job *j, WinSlot &s) {
+    const uint64_t S = 2 * j->nm_cap;
+    int rc;
+    if ((rc = dalloc(j, &s.d_ms, j->nm_cap)) || (rc = dalloc(j, &s.d_rank, j->nodd_cap)) ||
+        (rc = dalloc(j, &s.d_bitmaps, j->nm_cap * j->W)) || (rc = dalloc(j, &s.d_lists, S * j->cap)) ||
+        (rc = dalloc(j, &s.d_counts, S)) || (rc = dalloc(j, &s.d_found, S)) || (rc = dalloc(j, &s.d_kstart, S)) ||
+        (rc = dalloc(j, &s.d_knext, S)) || (rc = dalloc(j, &s.d_gaps, S)) || (rc = dalloc(j, &s.d_act0, S)) ||
+        (rc = dalloc(j, &s.d_act1, S)) || (rc = dalloc(j, &s.d_redo, S)) || (rc = dalloc(j, &s.d_sc, 1)))
+        return rc;
+    PG_CUDA(cudaMallocHost((void **)&s.h_sc, sizeof(Scalars)));
+    PG_CUDA(cudaMallocHost((void **)&s.h_ms, j->nm_cap * 8));
+    PG_CUDA(cudaMallocHost((void **)&s.h_rank, j->nodd_cap * 4));
+    PG_CUDA(cudaMallocHost((void **)&s.h_gaps, S * 4));
+    for (auto &e : s.ev) PG_CUDA(cudaEventCreate(&e));
+    PG_CUDA(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
+    return PG_OK;
+}
 
 static int job_build(pg_job *j) {
     const pg_job_params &p = j->prm;
@@ -474,24 +507,15 @@ static int job_build(pg_job *j) {
         cudaFree(d_cnt);
         cudaFree(d_off);
     }
-    // ---- window buffers
+    // ---- window slots
     const uint64_t mi = std::max<uint64_t>(p.max_m_inc, 2);
     j->nodd_cap = mi / 2 + 1;
     uint64_t phi = 0;
     for (uint64_t r = 1; r <= p.d; r++) phi += gcd64(r, p.d) == 1;
     j->nm_cap = std::min<uint64_t>(j->nodd_cap, (mi / p.d + 1) * phi);
     if (2 * j->nm_cap >= 0xffffffffull) return fail(PG_ERR_UNSUPPORTED, "max_m_inc too large");
-    const uint64_t S = 2 * j->nm_cap;
-    if ((rc = dalloc(j, &j->d_ms, j->nm_cap)) || (rc = dalloc(j, &j->d_rank, j->nodd_cap)) ||
-        (rc = dalloc(j, &j->d_bitmaps, j->nm_cap * j->W)) || (rc = dalloc(j, &j->d_lists, S * j->cap)) ||
-        (rc = dalloc(j, &j->d_counts, S)) || (rc = dalloc(j, &j->d_found, S)) || (rc = dalloc(j, &j->d_kstart, S)) ||
-        (rc = dalloc(j, &j->d_knext, S)) || (rc = dalloc(j, &j->d_gaps, S)) || (rc = dalloc(j, &j->d_act0, S)) ||
-        (rc = dalloc(j, &j->d_act1, S)) || (rc = dalloc(j, &j->d_redo, S)) || (rc = dalloc(j, &j->d_sc, 1)))
-        return rc;
-    PG_CUDA(cudaMallocHost((void **)&j->h_sc, sizeof(Scalars)));
-    PG_CUDA(cudaMallocHost((void **)&j->h_ms, j->nm_cap * 8));
-    PG_CUDA(cudaMallocHost((void **)&j->h_rank, j->nodd_cap * 4));
-    for (auto &e : j->ev) PG_CUDA(cudaEventCreate(&e));
+    for (auto &s : j->slot)
+        if ((rc = slot_alloc(j, s))) return rc;
     j->grid = search_grid(j->L, j->ctx->device);
     return PG_OK;
 }
@@ -545,109 +569,123 @@ extern "C" int pg_job_k_words(const pg_job *j, uint32_t *out, uint32_t *nwords) 
     return PG_OK;
 }
 
+extern "C" void *pg_job_stream(pg_job *j, int slot) {
+    if (!j || slot < 0 || slot >= PG_SEARCH_SLOTS) return nullptr;
+    return (void *)j->slot[slot].st;
+}
+
 // ============================================================== windows
 
-// Uploads the coprime m and the odd-m rank table of a window; returns the
-// number of coprime m in *nm.
-static int window_setup(pg_job *j, uint64_t m_start, uint64_t m_inc, uint64_t *m0, uint64_t *nodd, uint32_t *nm) {
+// Computes the coprime m and the odd-m rank table of a window into the
+// slot's pinned staging and uploads them on the slot's stream.
+static int window_setup(pg_job *j, WinSlot &s, uint64_t m_start, uint64_t m_inc) {
     const pg_job_params &p = j->prm;
     if (m_inc == 0) return fail(PG_ERR_ARG, "m_inc must be > 0");
-    if (m_inc > std::max<uint64_t>(p.max_m_inc, 2)) return fail(PG_ERR_ARG, "m_inc=%llu > max_m_inc=%llu",
-                                                                 (unsigned long long)m_inc,
-                                                                 (unsigned long long)p.max_m_inc);
-    if (m_start + m_inc - 1 > p.max_m) return fail(PG_ERR_ARG, "m beyond max_m");
+    if (m_inc > std::max<uint64_t>(p.max_m_inc, 2))
+        return fail(PG_ERR_ARG, "m_inc=%llu > max_m_inc=%llu", (unsigned long long)m_inc,
+                    (unsigned long long)p.max_m_inc);
     if (m_start == 0) return fail(PG_ERR_ARG, "m_start must be > 0");
-    cudaStream_t st = j->ctx->stream;
-    PG_CUDA(cudaStreamSynchronize(st));  // pinned staging is reused
-    *m0 = m_start | 1ull;
+    if (m_start + m_inc - 1 > p.max_m) return fail(PG_ERR_ARG, "m beyond max_m");
+    s.m0 = m_start | 1ull;
     const uint64_t end = m_start + m_inc;
-    *nodd = end > *m0 ? (end - *m0 + 1) / 2 : 0;
+    s.nodd = end > s.m0 ? (end - s.m0 + 1) / 2 : 0;
     uint32_t r = 0;
-    for (uint64_t jj = 0; jj < *nodd; jj++) {
-        const uint64_t m = *m0 + 2 * jj;
+    for (uint64_t jj = 0; jj < s.nodd; jj++) {
+        const uint64_t m = s.m0 + 2 * jj;
         if (gcd64(m, p.d) == 1) {
-            j->h_ms[r] = m;
-            j->h_rank[jj] = (int32_t)r++;
+            s.h_ms[r] = m;
+            s.h_rank[jj] = (int32_t)r++;
         } else {
-            j->h_rank[jj] = -1;
+            s.h_rank[jj] = -1;
         }
     }
-    *nm = r;
-    if (r) PG_CUDA(cudaMemcpyAsync(j->d_ms, j->h_ms, (size_t)r * 8, cudaMemcpyHostToDevice, st));
-    if (*nodd) PG_CUDA(cudaMemcpyAsync(j->d_rank, j->h_rank, (size_t)*nodd * 4, cudaMemcpyHostToDevice, st));
+    s.nm = r;
+    if (r) PG_CUDA(cudaMemcpyAsync(s.d_ms, s.h_ms, (size_t)r * 8, cudaMemcpyHostToDevice, s.st));
+    if (s.nodd) PG_CUDA(cudaMemcpyAsync(s.d_rank, s.h_rank, (size_t)s.nodd * 4, cudaMemcpyHostToDevice, s.st));
     return PG_OK;
 }
 
 // First prime-table index sieved by modular search rather than by stepping
 // every Y: primes whose expected hits in the window, nodd * (2 sly + 1) / p,
-// fall below LARGE_SEARCH_HITS (the two methods cost about the same there).
-static constexpr double LARGE_SEARCH_HITS = 16.0;
-
+// fall below search_hits (default 64; the measured crossover of the two
+// methods on the P=503 window is between 32 and 128).
 static uint64_t large_split(const pg_job *j, uint64_t nodd) {
     if (j->np == 0) return 0;
     if (j->prm.flags & PG_JOB_LARGE_STEP) return j->np;
     if (j->prm.flags & PG_JOB_LARGE_SEARCH) return 0;
-    const double pv = (double)nodd * (2.0 * j->sly + 1) / LARGE_SEARCH_HITS;
+    const double hits = j->prm.search_hits ? (double)j->prm.search_hits : 64.0;
+    const double pv = (double)nodd * (2.0 * j->sly + 1) / hits;
     if (pv <= (double)j->seg_v0) return 0;
     const double s = (pv - (double)j->seg_v0) / (double)j->seg_span;
     if (s >= (double)j->seg_off.size()) return j->np;
     return j->seg_off[(size_t)s];
 }
 
-static int run_sieve(pg_job *j, uint64_t m0, uint64_t nodd, uint32_t nm, bool compact) {
-    cudaStream_t st = j->ctx->stream;
-    PG_CUDA(cudaMemsetAsync(j->d_bitmaps, 0, (size_t)nm * j->W * 4, st));
-    PG_CUDA(cudaMemsetAsync(j->d_sc, 0, sizeof(Scalars), st));
+static int run_sieve(pg_job *j, WinSlot &s, bool compact) {
+    PG_CUDA(cudaMemsetAsync(s.d_bitmaps, 0, (size_t)s.nm * j->W * 4, s.st));
+    PG_CUDA(cudaMemsetAsync(&s.d_sc->max_count, 0, 4, s.st));
     LargeArgs la{};
     la.sly = j->sly;
     la.words = j->W;
-    la.m0 = m0;
-    la.nodd = nodd;
-    la.rank = j->d_rank;
-    la.bitmaps = j->d_bitmaps;
+    la.m0 = s.m0;
+    la.nodd = s.nodd;
+    la.rank = s.d_rank;
+    la.bitmaps = s.d_bitmaps;
     la.np = j->np;
     la.p = j->d_lp;
     la.cinv = j->d_lcinv;
     la.c = j->d_lc;
-    PG_CUDA(launch_sieve_large(la, j->wide, large_split(j, nodd), st));
+    const uint64_t split = large_split(j, s.nodd);
+    PG_CUDA(launch_sieve_large(la, j->wide, split, s.st));
+    s.sst.kernel_launches += (split > 0) + (split < j->np);
     SieveArgs sa{};
     sa.sly = j->sly;
     sa.words = j->W;
     sa.cap = j->cap;
-    sa.m0 = m0;
-    sa.nodd = nodd;
-    sa.nm = nm;
-    sa.ms = j->d_ms;
-    sa.rank = j->d_rank;
-    sa.bitmaps = j->d_bitmaps;
+    sa.m0 = s.m0;
+    sa.nodd = s.nodd;
+    sa.nm = s.nm;
+    sa.ms = s.d_ms;
+    sa.rank = s.d_rank;
+    sa.bitmaps = s.d_bitmaps;
     sa.wheel = j->d_wheel;
     sa.sq = j->d_sq;
     sa.sr = j->d_sr;
     sa.sbar = j->d_sbar;
     sa.nsmall = j->nsmall;
-    sa.lists = j->d_lists;
-    sa.counts = j->d_counts;
-    sa.max_count = &j->d_sc->max_count;
-    PG_CUDA(launch_sieve_small(sa, compact, st));
+    sa.lists = s.d_lists;
+    sa.counts = s.d_counts;
+    sa.max_count = &s.d_sc->max_count;
+    PG_CUDA(launch_sieve_small(sa, compact, s.st));
+    s.sst.kernel_launches++;
+    return PG_OK;
+}
+
+static int slot_idle(pg_job *j, WinSlot &s, const char *who) {
+    if (s.busy)
+        return fail(PG_ERR_STATE, "%s: window slot holds ticket %llu; pg_search_wait it first", who,
+                    (unsigned long long)s.ticket);
+    (void)j;
     return PG_OK;
 }
 
 extern "C" int pg_sieve_interval(pg_job *j, uint64_t m_start, uint64_t m_inc, uint64_t *ms, uint32_t *bitmaps) {
     if (!j) return fail(PG_ERR_ARG, "pg_sieve_interval: job is NULL");
     PG_CUDA(cudaSetDevice(j->ctx->device));
-    uint64_t m0, nodd;
-    uint32_t nm;
-    int rc = window_setup(j, m_start, m_inc, &m0, &nodd, &nm);
+    WinSlot &s = j->slot[0];
+    int rc = slot_idle(j, s, "pg_sieve_interval");
     if (rc) return rc;
-    if ((rc = run_sieve(j, m0, nodd, nm, false))) return rc;
-    cudaStream_t st = j->ctx->stream;
-    if (bitmaps && nm) PG_CUDA(cudaMemcpyAsync(bitmaps, j->d_bitmaps, (size_t)nm * j->W * 4, cudaMemcpyDeviceToHost, st));
-    PG_CUDA(cudaStreamSynchronize(st));
-    if (ms) std::memcpy(ms, j->h_ms, (size_t)nm * 8);
+    PG_CUDA(cudaStreamSynchronize(s.st));  // pinned staging is reused
+    if ((rc = window_setup(j, s, m_start, m_inc))) return rc;
+    if ((rc = run_sieve(j, s, false))) return rc;
+    if (bitmaps && s.nm)
+        PG_CUDA(cudaMemcpyAsync(bitmaps, s.d_bitmaps, (size_t)s.nm * j->W * 4, cudaMemcpyDeviceToHost, s.st));
+    PG_CUDA(cudaStreamSynchronize(s.st));
+    if (ms) std::memcpy(ms, s.h_ms, (size_t)s.nm * 8);
     return PG_OK;
 }
 
-static SearchArgs base_args(pg_job *j) {
+static SearchArgs base_args(pg_job *j, WinSlot &s) {
     SearchArgs a{};
     std::memset(a.K, 0, sizeof a.K);
     std::memcpy(a.K, j->K.data(), j->K.size() * 4);
@@ -656,133 +694,181 @@ static SearchArgs base_args(pg_job *j) {
     a.cap = j->cap;
     a.ntrial = TRIAL_PRIMES;
     a.rounds = j->prm.rounds;
-    a.ms = j->d_ms;
-    a.lists = j->d_lists;
-    a.counts = j->d_counts;
-    a.k_start = j->d_kstart;
-    a.found_k = j->d_found;
-    a.next_item = &j->d_sc->next_item;
-    a.tests = &j->d_sc->tests;
+    a.ms = s.d_ms;
+    a.lists = s.d_lists;
+    a.counts = s.d_counts;
+    a.k_start = s.d_kstart;
+    a.found_k = s.d_found;
+    a.next_item = &s.d_sc->next_item;
+    a.tests = &s.d_sc->tests;
     a.trial_q = j->d_tq;
     a.trial_r = j->d_tr;
     return a;
 }
 
-extern "C" int pg_search(pg_job *j, uint64_t m_start, uint64_t m_inc, int form, uint64_t *ms, uint32_t *prev_gap,
-                         uint32_t *next_gap, pg_search_stats *stats) {
-    if (!j) return fail(PG_ERR_ARG, "pg_search: job is NULL");
-    if (form != PG_SEARCH_PERSISTENT && form != PG_SEARCH_PLAIN) return fail(PG_ERR_ARG, "pg_search: form=%d", form);
+// Finalize all sides and queue the copies back; the host reads n_redo in
+// slot_finish.
+static int enqueue_finalize(pg_job *j, WinSlot &s, SearchArgs &a, uint32_t S) {
+    PG_CUDA(cudaMemsetAsync(&s.d_sc->n_redo, 0, 4, s.st));
+    PG_CUDA(launch_finalize(j->L, a, S, s.d_gaps, s.d_redo, &s.d_sc->n_redo, &s.d_sc->confirm, s.d_kstart, s.st));
+    s.sst.kernel_launches++;
+    PG_CUDA(cudaEventRecord(s.ev[2], s.st));  // end of the device work (before the copies back)
+    PG_CUDA(cudaMemcpyAsync(s.h_gaps, s.d_gaps, (size_t)S * 4, cudaMemcpyDeviceToHost, s.st));
+    PG_CUDA(cudaMemcpyAsync(s.h_sc, s.d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s.st));
+    return PG_OK;
+}
+
+extern "C" int pg_search_submit(pg_job *j, uint64_t m_start, uint64_t m_inc, int form, uint32_t flags,
+                                uint64_t *ticket) {
+    if (!j || !ticket) return fail(PG_ERR_ARG, "pg_search_submit: NULL argument");
+    if (form != PG_SEARCH_PERSISTENT && form != PG_SEARCH_PLAIN)
+        return fail(PG_ERR_ARG, "pg_search_submit: form=%d", form);
     PG_CUDA(cudaSetDevice(j->ctx->device));
-    cudaStream_t st = j->ctx->stream;
-    uint64_t m0, nodd;
-    uint32_t nm;
-    int rc = window_setup(j, m_start, m_inc, &m0, &nodd, &nm);
+    WinSlot &s = j->slot[j->next_ticket % PG_SEARCH_SLOTS];
+    int rc = slot_idle(j, s, "pg_search_submit");
     if (rc) return rc;
-    pg_search_stats sst{};
-    sst.m_count = nm;
-    sst.h2d_bytes = (uint64_t)nm * 8 + (uint64_t)nodd * 4;
-    if (nm == 0) {
-        if (stats) *stats = sst;
-        return PG_OK;
-    }
-    const uint32_t S = 2 * nm;
-    PG_CUDA(cudaEventRecord(j->ev[0], st));
-    if ((rc = run_sieve(j, m0, nodd, nm, true))) return rc;
-    sst.kernel_launches += (j->np ? 1 : 0) + 1;
-    PG_CUDA(cudaEventRecord(j->ev[1], st));
-    PG_CUDA(cudaMemsetAsync(j->d_found, 0xff, (size_t)S * 4, st));
-    PG_CUDA(cudaMemsetAsync(j->d_kstart, 0, (size_t)S * 4, st));
-    PG_CUDA(launch_iota(j->d_act0, S, st));
-    sst.kernel_launches++;
-    SearchArgs a = base_args(j);
-    a.act = j->d_act0;
+    PG_CUDA(cudaStreamSynchronize(s.st));  // the slot's pinned staging is reused
+    s.sst = pg_search_stats{};
+    if ((rc = window_setup(j, s, m_start, m_inc))) return rc;
+    s.sst.m_count = s.nm;
+    s.sst.h2d_bytes = (uint64_t)s.nm * 8 + (uint64_t)s.nodd * 4;
+    s.ticket = j->next_ticket++;
+    s.busy = true;
+    *ticket = s.ticket;
+    if (s.nm == 0) return PG_OK;
+    const uint32_t S = 2 * s.nm;
+    PG_CUDA(cudaEventRecord(s.ev[0], s.st));
+    if ((rc = run_sieve(j, s, true))) return rc;
+    PG_CUDA(cudaEventRecord(s.ev[1], s.st));
+    const uint32_t warps = (uint32_t)j->grid * 4;
+    PG_CUDA(launch_init_search(S, s.d_found, s.d_kstart, s.d_act0, s.d_sc, warps, s.st));
+    s.sst.kernel_launches++;
+    SearchArgs a = base_args(j, s);
+    a.act = s.d_act0;
     a.n_act = S;
     a.ext_max = j->prm.ext_window;
     if (form == PG_SEARCH_PERSISTENT) {
         a.kspan = j->cap + a.ext_max;
-        a.max_count = &j->d_sc->max_count;
-        PG_CUDA(cudaEventRecord(j->ev[3], st));
-        PG_CUDA(launch_search_persistent(j->L, a, j->grid, st));
-        PG_CUDA(cudaEventRecord(j->ev[4], st));
-        sst.kernel_launches++;
-        sst.passes = 1;
-    } else {
-        PG_CUDA(cudaMemsetAsync(j->d_knext, 0, (size_t)S * 4, st));
+        a.max_count = &s.d_sc->max_count;
+        a.unresolved = &s.d_sc->unresolved;
+        a.active_warps = &s.d_sc->active_warps;
+        if (flags & PG_SUBMIT_DRAIN) {
+            a.drain_lanes = 4;
+            a.min_warps = (uint32_t)j->ctx->sms;
+        }
+        PG_CUDA(cudaEventRecord(s.ev[3], s.st));
+        PG_CUDA(launch_search_persistent(j->L, a, j->grid, s.st));
+        PG_CUDA(cudaEventRecord(s.ev[4], s.st));
+        s.sst.kernel_launches++;
+        s.sst.passes = 1;
+    } else {  // one launch per pass, the active-side count read back after each
+        PG_CUDA(cudaMemsetAsync(s.d_knext, 0, (size_t)S * 4, s.st));
         uint32_t n_act = S;
-        uint32_t *cur = j->d_act0, *nxt = j->d_act1;
-        PG_CUDA(cudaEventRecord(j->ev[3], st));
+        uint32_t *cur = s.d_act0, *nxt = s.d_act1;
+        PG_CUDA(cudaEventRecord(s.ev[3], s.st));
         while (n_act > 0) {
             a.act = cur;
             a.n_act = n_act;
-            PG_CUDA(launch_search_plain(j->L, a, j->d_knext, st));
-            sst.passes++;
-            PG_CUDA(cudaMemsetAsync(&j->d_sc->n_out, 0, 4, st));
-            PG_CUDA(launch_compact_active(cur, n_act, j->d_found, j->d_knext, j->d_counts, a.ext_max, nxt,
-                                          &j->d_sc->n_out, st));
-            sst.kernel_launches += 2;
-            sst.d2h_bytes += 4;
-            PG_CUDA(cudaMemcpyAsync(&j->h_sc->n_out, &j->d_sc->n_out, 4, cudaMemcpyDeviceToHost, st));
-            PG_CUDA(cudaStreamSynchronize(st));
-            n_act = j->h_sc->n_out;
+            PG_CUDA(launch_search_plain(j->L, a, s.d_knext, s.st));
+            s.sst.passes++;
+            PG_CUDA(cudaMemsetAsync(&s.d_sc->n_out, 0, 4, s.st));
+            PG_CUDA(launch_compact_active(cur, n_act, s.d_found, s.d_knext, s.d_counts, a.ext_max, nxt,
+                                          &s.d_sc->n_out, s.st));
+            s.sst.kernel_launches += 2;
+            s.sst.d2h_bytes += 4;
+            PG_CUDA(cudaMemcpyAsync(&s.h_sc->n_out, &s.d_sc->n_out, 4, cudaMemcpyDeviceToHost, s.st));
+            PG_CUDA(cudaStreamSynchronize(s.st));
+            n_act = s.h_sc->n_out;
             std::swap(cur, nxt);
         }
-        PG_CUDA(cudaEventRecord(j->ev[4], st));
-        PG_CUDA(launch_iota(j->d_act0, S, st));
-        sst.kernel_launches++;
+        PG_CUDA(cudaEventRecord(s.ev[4], s.st));
+        PG_CUDA(launch_iota(s.d_act0, S, s.st));
+        s.sst.kernel_launches++;
     }
-    // finalize every side, then continue the unresolved ones on the device
-    a.act = j->d_act0;
+    a.act = s.d_act0;
     a.n_act = S;
     a.max_count = nullptr;
-    uint32_t ext_done = a.ext_max;
+    return enqueue_finalize(j, s, a, S);
+}
+
+// Waits for the slot's queued work; continues sides without a prime within
+// sl + ext_window on the device with 4x larger extension windows.
+static int slot_finish(pg_job *j, WinSlot &s) {
+    PG_CUDA(cudaStreamSynchronize(s.st));
+    const uint32_t S = 2 * s.nm;
+    SearchArgs a = base_args(j, s);
+    uint32_t ext_done = j->prm.ext_window;
     for (int round = 0;; round++) {
-        PG_CUDA(cudaMemsetAsync(&j->d_sc->n_redo, 0, 4, st));
-        PG_CUDA(launch_finalize(j->L, a, S, j->d_gaps, j->d_redo, &j->d_sc->n_redo, &j->d_sc->confirm, j->d_kstart, st));
-        sst.kernel_launches++;
-        sst.d2h_bytes += 4;
-        PG_CUDA(cudaMemcpyAsync(&j->h_sc->n_redo, &j->d_sc->n_redo, 4, cudaMemcpyDeviceToHost, st));
-        PG_CUDA(cudaStreamSynchronize(st));
-        const uint32_t n_redo = j->h_sc->n_redo;
+        const uint32_t n_redo = s.h_sc->n_redo;
         if (n_redo == 0) break;
-        if (round >= 24) return fail(PG_ERR_STATE, "pg_search: %u sides unresolved after %u extension positions", n_redo,
-                                     ext_done);
-        // continuation: the redo list becomes the active list
-        PG_CUDA(cudaMemcpyAsync(j->d_act1, j->d_redo, (size_t)n_redo * 4, cudaMemcpyDeviceToDevice, st));
+        if (round >= 24)
+            return fail(PG_ERR_STATE, "pg_search: %u sides unresolved after %u extension positions", n_redo, ext_done);
+        PG_CUDA(cudaMemcpyAsync(s.d_act1, s.d_redo, (size_t)n_redo * 4, cudaMemcpyDeviceToDevice, s.st));
         const uint32_t ext_new = std::min<uint32_t>(ext_done * 4, 1u << 26);
-        a.act = j->d_act1;
+        a.act = s.d_act1;
         a.n_act = n_redo;
         a.ext_max = ext_new;
         a.kspan = j->cap + ext_new;
-        PG_CUDA(cudaMemsetAsync(&j->d_sc->next_item, 0, 8, st));
-        PG_CUDA(launch_search_persistent(j->L, a, j->grid, st));
-        sst.kernel_launches++;
-        sst.relaunches++;
-        sst.extended_sides += n_redo;
+        a.max_count = nullptr;
+        PG_CUDA(cudaMemsetAsync(&s.d_sc->next_item, 0, 8, s.st));
+        PG_CUDA(launch_search_persistent(j->L, a, j->grid, s.st));
+        s.sst.kernel_launches++;
+        s.sst.relaunches++;
+        s.sst.extended_sides += n_redo;
         ext_done = ext_new;
+        // finalize the continued sides only (their gaps and a new redo list)
+        PG_CUDA(cudaMemsetAsync(&s.d_sc->n_redo, 0, 4, s.st));
+        PG_CUDA(launch_finalize(j->L, a, S, s.d_gaps, s.d_redo, &s.d_sc->n_redo, &s.d_sc->confirm, s.d_kstart, s.st));
+        s.sst.kernel_launches++;
+        PG_CUDA(cudaEventRecord(s.ev[2], s.st));
+        PG_CUDA(cudaMemcpyAsync(s.h_gaps, s.d_gaps, (size_t)S * 4, cudaMemcpyDeviceToHost, s.st));
+        PG_CUDA(cudaMemcpyAsync(s.h_sc, s.d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s.st));
+        s.sst.d2h_bytes += 4;
+        PG_CUDA(cudaStreamSynchronize(s.st));
     }
-    PG_CUDA(cudaEventRecord(j->ev[2], st));
-    std::vector<uint32_t> gaps(S);
-    PG_CUDA(cudaMemcpyAsync(gaps.data(), j->d_gaps, (size_t)S * 4, cudaMemcpyDeviceToHost, st));
-    PG_CUDA(cudaMemcpyAsync(j->h_sc, j->d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
-    PG_CUDA(cudaStreamSynchronize(st));
-    for (uint32_t r = 0; r < nm; r++) {
-        if (next_gap) next_gap[r] = gaps[2 * r];
-        if (prev_gap) prev_gap[r] = gaps[2 * r + 1];
-    }
-    if (ms) std::memcpy(ms, j->h_ms, (size_t)nm * 8);
-    sst.d2h_bytes += (uint64_t)S * 4 + sizeof(Scalars);
-    float t_sieve = 0, t_prp = 0, t_kernel = 0;
-    cudaEventElapsedTime(&t_sieve, j->ev[0], j->ev[1]);
-    cudaEventElapsedTime(&t_prp, j->ev[1], j->ev[2]);
-    cudaEventElapsedTime(&t_kernel, j->ev[3], j->ev[4]);
-    sst.search_kernel_ms = t_kernel;
-    sst.sieve_ms = t_sieve;
-    sst.prp_ms = t_prp;
-    sst.total_ms = t_sieve + t_prp;
-    sst.prp_tests = j->h_sc->tests;
-    sst.confirm_tests = j->h_sc->confirm;
-    if (stats) *stats = sst;
     return PG_OK;
+}
+
+extern "C" int pg_search_wait(pg_job *j, uint64_t ticket, uint64_t *ms, uint32_t *prev_gap, uint32_t *next_gap,
+                              pg_search_stats *stats) {
+    if (!j) return fail(PG_ERR_ARG, "pg_search_wait: job is NULL");
+    PG_CUDA(cudaSetDevice(j->ctx->device));
+    WinSlot &s = j->slot[ticket % PG_SEARCH_SLOTS];
+    if (!s.busy || s.ticket != ticket)
+        return fail(PG_ERR_STATE, "pg_search_wait: ticket %llu is not in flight", (unsigned long long)ticket);
+    s.busy = false;
+    if (s.nm == 0) {
+        if (stats) *stats = s.sst;
+        return PG_OK;
+    }
+    int rc = slot_finish(j, s);
+    if (rc) return rc;
+    for (uint32_t r = 0; r < s.nm; r++) {
+        if (next_gap) next_gap[r] = s.h_gaps[2 * r];
+        if (prev_gap) prev_gap[r] = s.h_gaps[2 * r + 1];
+    }
+    if (ms) std::memcpy(ms, s.h_ms, (size_t)s.nm * 8);
+    s.sst.d2h_bytes += (uint64_t)2 * s.nm * 4 + sizeof(Scalars);
+    float t_sieve = 0, t_prp = 0, t_kernel = 0;
+    cudaEventElapsedTime(&t_sieve, s.ev[0], s.ev[1]);
+    cudaEventElapsedTime(&t_prp, s.ev[1], s.ev[2]);
+    cudaEventElapsedTime(&t_kernel, s.ev[3], s.ev[4]);
+    s.sst.search_kernel_ms = t_kernel;
+    s.sst.sieve_ms = t_sieve;
+    s.sst.prp_ms = t_prp;
+    s.sst.total_ms = t_sieve + t_prp;
+    s.sst.prp_tests = s.h_sc->tests;
+    s.sst.confirm_tests = s.h_sc->confirm;
+    if (stats) *stats = s.sst;
+    return PG_OK;
+}
+
+extern "C" int pg_search(pg_job *j, uint64_t m_start, uint64_t m_inc, int form, uint64_t *ms, uint32_t *prev_gap,
+                         uint32_t *next_gap, pg_search_stats *stats) {
+    uint64_t t = 0;
+    int rc = pg_search_submit(j, m_start, m_inc, form, 0, &t);
+    if (rc) return rc;
+    return pg_search_wait(j, t, ms, prev_gap, next_gap, stats);
 }
 
 // ============================================================= records

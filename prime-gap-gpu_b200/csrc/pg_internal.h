@@ -37,6 +37,25 @@ struct SearchArgs {
     unsigned long long *tests;      // PRP tests executed
     const uint32_t *trial_q;   // [TRIAL_PRIMES] 3, 5, 7, ...
     const uint32_t *trial_r;   // [TRIAL_PRIMES] (-(K mod q)/2) mod q
+    // draining: a warp with no work in hand retires when more than
+    // drain_lanes lanes per unresolved side are active (0 = never retire)
+    uint32_t *unresolved;      // sides of this launch without a probable prime yet
+    uint32_t *active_warps;    // warps of this launch still pulling work
+    uint32_t drain_lanes;
+    uint32_t min_warps;        // never retire below this many warps
+};
+
+// Device scalars of one window slot.
+struct Scalars {
+    unsigned long long next_item;
+    unsigned long long tests;
+    unsigned long long confirm;
+    uint32_t n_redo;
+    uint32_t n_out;
+    uint32_t max_count;
+    uint32_t unresolved;
+    uint32_t active_warps;
+    uint32_t pad;
 };
 
 // Arguments of the sieve kernels for one window.
@@ -94,6 +113,10 @@ cudaError_t launch_finalize(uint32_t L, const SearchArgs &a, uint32_t nsides, ui
                             uint32_t *redo, uint32_t *n_redo, unsigned long long *confirm_tests,
                             uint32_t *k_start_rw, cudaStream_t st);
 cudaError_t launch_iota(uint32_t *out, uint32_t n, cudaStream_t st);
+// found_k = NOT_FOUND, k_start = 0, act = 0..S-1 for S sides; the scalars'
+// queue head and counters = 0, unresolved = S, active_warps = warps
+cudaError_t launch_init_search(uint32_t S, uint32_t *found_k, uint32_t *k_start, uint32_t *act, Scalars *sc,
+                               uint32_t warps, cudaStream_t st);
 cudaError_t launch_imad_peak(int grid, uint32_t iters, uint32_t *sink, cudaStream_t st);
 // records the calling thread's pg_last_error() text (pg_api.cu)
 void set_error(const char *msg);

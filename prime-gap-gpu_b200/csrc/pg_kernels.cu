@@ -518,6 +518,31 @@ __global__ void k_iota(uint32_t *out, uint32_t n) {
     if (i < n) out[i] = i;
 }
 
+__global__ void k_init_search(uint32_t S, uint32_t *found_k, uint32_t *k_start, uint32_t *act, Scalars *sc,
+                              uint32_t warps) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < S) {
+        found_k[i] = NOT_FOUND;
+        k_start[i] = 0;
+        act[i] = i;
+    }
+    if (i == 0) {
+        sc->next_item = 0;
+        sc->tests = 0;
+        sc->confirm = 0;
+        sc->n_redo = 0;
+        sc->n_out = 0;
+        sc->unresolved = S;
+        sc->active_warps = warps;
+    }
+}
+
+cudaError_t launch_init_search(uint32_t S, uint32_t *found_k, uint32_t *k_start, uint32_t *act, Scalars *sc,
+                               uint32_t warps, cudaStream_t st) {
+    k_init_search<<<(S + 255) / 256 + 1, 256, 0, st>>>(S, found_k, k_start, act, sc, warps);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_iota(uint32_t *out, uint32_t n, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     k_iota<<<(n + 255) / 256, 256, 0, st>>>(out, n);

@@ -15,6 +15,12 @@
 #include "pg_internal.h"
 #include "pg_mont.cuh"
 
+// minimum resident 128-thread blocks per SM requested from ptxas for the
+// persistent search (caps its registers); 1 leaves the choice to ptxas
+#ifndef PG_PERSIST_MIN_BLOCKS
+#define PG_PERSIST_MIN_BLOCKS 1
+#endif
+
 namespace pg {
 
 // ================================================================= PRP
@@ -108,7 +114,7 @@ __device__ __forceinline__ uint32_t item_y(const SearchArgs &a, uint32_t s, uint
 // A side is resolved by the smallest k with a probable prime: every smaller
 // k is tested because items are only skipped behind a smaller found k.
 template <int L>
-__global__ void __launch_bounds__(128) k_search_persistent(const __grid_constant__ SearchArgs a) {
+__global__ void __launch_bounds__(128, PG_PERSIST_MIN_BLOCKS) k_search_persistent(const __grid_constant__ SearchArgs a) {
     const unsigned FULL = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31;
     uint32_t kspan = a.kspan;
@@ -118,6 +124,24 @@ __global__ void __launch_bounds__(128) k_search_persistent(const __grid_constant
     uint32_t s = 0, k = 0, Y = 0;
     unsigned long long ntests = 0;
     while (true) {
+        // Draining: once the unresolved sides are few, extra lanes would only
+        // test candidates beyond a prime about to be found; such a warp leaves
+        // (with no item in hand) so its SM slot can run other work.  The last
+        // min_warps warps never leave, so every item is still handed out.
+        if (a.drain_lanes && !exhausted) {
+            int retire = 0;
+            if (lane == 0) {
+                const uint32_t u = *(volatile const uint32_t *)a.unresolved;
+                const uint32_t w = *(volatile const uint32_t *)a.active_warps;
+                if ((unsigned long long)u * a.drain_lanes < (unsigned long long)w * 32 && w > a.min_warps) {
+                    if (atomicSub(a.active_warps, 1u) > a.min_warps)
+                        retire = 1;
+                    else
+                        atomicAdd(a.active_warps, 1u);
+                }
+            }
+            if (__shfl_sync(FULL, retire, 0)) break;
+        }
         while (!exhausted) {
             const unsigned need = __ballot_sync(FULL, !have);
             if (need == 0) break;
@@ -146,7 +170,7 @@ __global__ void __launch_bounds__(128) k_search_persistent(const __grid_constant
             build_candidate<L>(a, a.ms[s >> 1], Y, s & 1, x);
             const bool pr = strong_prp<L>(x, 2);
             ntests++;
-            if (pr) atomicMin(&a.found_k[s], k);
+            if (pr && atomicMin(&a.found_k[s], k) == NOT_FOUND && a.unresolved) atomicSub(a.unresolved, 1u);
             have = false;
         }
     }

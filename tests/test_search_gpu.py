@@ -105,6 +105,38 @@ def test_odd_start_and_small_windows(pg, oracle):
             assert np.array_equal(res.prev_gap, prev) and np.array_equal(res.next_gap, nxt)
 
 
+@pytest.mark.parametrize("flags", [0, 1])  # 1 = PG_SUBMIT_DRAIN
+def test_pipelined_windows_equal_synchronous(pg, flags):
+    windows = [(1_000_000, 20_000), (1_020_000, 20_000), (1_040_000, 7_001), (1_000_000, 20_000)]
+    with pg.Job(503, 2190, 10_000, 50_000_000, max_m_inc=20_000, max_m=2_000_000) as job:
+        want = [job.search(a, b) for a, b in windows]
+        got, pending = [], []
+        for a, b in windows:
+            pending.append(job.submit(a, b, pg.PG_SEARCH_PERSISTENT, flags))
+            if len(pending) == pg.PG_SEARCH_SLOTS:
+                got.append(job.wait(pending.pop(0)))
+        while pending:
+            got.append(job.wait(pending.pop(0)))
+    for w, g in zip(want, got):
+        assert np.array_equal(w.ms, g.ms)
+        assert np.array_equal(w.prev_gap, g.prev_gap) and np.array_equal(w.next_gap, g.next_gap)
+
+
+def test_slot_state_errors(pg):
+    with pg.Job(337, 2310, 1_000, 1_000_000, max_m_inc=1_000, max_m=2 * 10**7) as job:
+        t0 = job.submit(10_000_000, 1_000)
+        t1 = job.submit(10_001_000, 1_000)
+        with pytest.raises(pg.PrimeGapError):
+            job.submit(10_002_000, 1_000)          # both slots hold un-waited tickets
+        with pytest.raises(pg.PrimeGapError):
+            job.sieve_interval(10_000_000, 1_000)  # slot 0 is busy
+        job.wait(t1)
+        job.wait(t0)
+        with pytest.raises(pg.PrimeGapError):
+            pg.lib.pg_search_wait(job._h, t0, None, None, None, None) and pg._check(-6)
+        assert len(job.search(10_000_000, 1_000).ms) == pg.count_m(10_000_000, 1_000, 2310)
+
+
 def test_repeat_is_deterministic(pg):
     with pg.Job(337, 2310, 7_500, 1_000_000, max_m_inc=3_000, max_m=2 * 10**7) as job:
         a = job.search(10_000_000, 3_000)
