@@ -108,7 +108,9 @@ typedef struct {
     uint32_t ext_window;   /* extension positions past sl tried in the first pass; 0 = 64 */
     uint32_t flags;        /* PG_JOB_* */
     uint32_t search_hits;  /* large primes expecting fewer hits per window than this are sieved
-                              by modular search, the others by stepping every X; 0 = 16 */
+                              by modular search, the others by stepping every X; 0 = 64 */
+    uint32_t tpi;          /* threads per number of the PRP kernels: 0 = automatic (one
+                              thread up to 48 words, then groups), 1, or a group size 4 / 8 */
 } pg_job_params;
 
 /* large-prime sieve: 0 = automatic, else force one method */
@@ -118,6 +120,7 @@ typedef struct {
 typedef struct {
     uint32_t k_bits;          /* bits of K */
     uint32_t limbs;           /* 32-bit words of the PRP operands */
+    uint32_t tpi;             /* threads per number of the PRP kernels */
     uint32_t words_per_m;     /* uint32 words of one sieve row */
     uint32_t side_capacity;   /* longest possible survivor list of one side */
     uint64_t num_primes;      /* primes in (P, max_prime] */

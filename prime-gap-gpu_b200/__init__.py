@@ -64,12 +64,14 @@ class JobParams(ctypes.Structure):
         ("max_prime", ctypes.c_uint64), ("max_m_inc", ctypes.c_uint64), ("max_m", ctypes.c_uint64),
         ("rounds", ctypes.c_uint32), ("small_limit", ctypes.c_uint32),
         ("ext_window", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("search_hits", ctypes.c_uint32),
+        ("tpi", ctypes.c_uint32),
     ]
 
 
 class JobInfo(ctypes.Structure):
     _fields_ = [
-        ("k_bits", ctypes.c_uint32), ("limbs", ctypes.c_uint32), ("words_per_m", ctypes.c_uint32),
+        ("k_bits", ctypes.c_uint32), ("limbs", ctypes.c_uint32), ("tpi", ctypes.c_uint32),
+        ("words_per_m", ctypes.c_uint32),
         ("side_capacity", ctypes.c_uint32), ("num_primes", ctypes.c_uint64), ("num_small", ctypes.c_uint64),
         ("k_log", ctypes.c_double), ("setup_seconds", ctypes.c_double), ("device_bytes", ctypes.c_uint64),
     ]
@@ -253,10 +255,10 @@ class Job:
 
     def __init__(self, p: int, d: int, sl: int, max_prime: int, max_m_inc: int, max_m: int,
                  rounds: int = 1, small_limit: int = 0, ext_window: int = 0, flags: int = 0,
-                 search_hits: int = 0, ctx: Context | None = None, device: int = 0):
+                 search_hits: int = 0, tpi: int = 0, ctx: Context | None = None, device: int = 0):
         self.ctx = ctx or Context(device)
         self.params = JobParams(p, d, sl, max_prime, max_m_inc, max_m, rounds, small_limit, ext_window, flags,
-                                search_hits)
+                                search_hits, tpi)
         h = ctypes.c_void_p()
         _check(lib.pg_job_create(self.ctx.handle, ctypes.byref(self.params), ctypes.byref(h)))
         self._h = h

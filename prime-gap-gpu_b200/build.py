@@ -42,6 +42,12 @@ def limb_list() -> list[int]:
     return [int(v) for v in re.findall(r"X\((\d+)\)", m.group(1))]
 
 
+def group_list() -> list[tuple[int, int]]:
+    text = (CSRC / "pg_limbs.h").read_text()
+    m = re.search(r"#define PG_GROUP_LIST\(X\)(.*)", text)
+    return [(int(a), int(b)) for a, b in re.findall(r"X\((\d+),\s*(\d+)\)", m.group(1))]
+
+
 def headers() -> list[pathlib.Path]:
     return sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "primegap.h"]
 
@@ -54,6 +60,8 @@ def units() -> list[tuple[pathlib.Path, pathlib.Path, list[str]]]:
             out.append((src, BUILD / f"{name}.o", []))
     for L in limb_list():
         out.append((CSRC / "pg_inst.cu", BUILD / f"pg_inst_{L}.o", [f"-DPG_LIMBS={L}"]))
+    for T, LT in group_list():
+        out.append((CSRC / "pg_ginst.cu", BUILD / f"pg_ginst_{T}x{LT}.o", [f"-DPG_GT={T}", f"-DPG_GLT={LT}"]))
     return out
 
 

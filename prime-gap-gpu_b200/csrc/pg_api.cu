@@ -390,9 +390,10 @@ static int job_build(pg_job *j) {
     }
     // ---- limbs of the PRP operands: N < K * (max_m + 1)
     const uint32_t nbits = j->kbits + bitlen64(p.max_m + 1);
-    const uint32_t words = (nbits + 31) / 32;
-    j->L = pick_limbs(words);
-    if (!j->L) return fail(PG_ERR_UNSUPPORTED, "operands of %u bits are above the compiled limit", nbits);
+    j->L = pick_layout(nbits, p.tpi);
+    if (!j->L)
+        return fail(PG_ERR_UNSUPPORTED, "operands of %u bits with tpi=%u are outside the compiled layouts", nbits,
+                    p.tpi);
     // ---- geometry
     j->sly = p.sl / 2;
     j->W = (2 * j->sly + 1 + 31) / 32;
@@ -551,7 +552,8 @@ extern "C" int pg_job_create(pg_ctx *c, const pg_job_params *params, pg_job **ou
 extern "C" int pg_job_get_info(const pg_job *j, pg_job_info *info) {
     if (!j || !info) return fail(PG_ERR_ARG, "pg_job_get_info: NULL argument");
     info->k_bits = j->kbits;
-    info->limbs = j->L;
+    info->limbs = layout_words(j->L);
+    info->tpi = j->L >> 16 ? j->L >> 16 : 1;
     info->words_per_m = j->W;
     info->side_capacity = j->cap;
     info->num_primes = j->np;

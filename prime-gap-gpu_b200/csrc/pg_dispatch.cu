@@ -1,29 +1,56 @@
-// pg_dispatch.cu -- maps a runtime limb count to its compiled instantiation.
+// pg_dispatch.cu -- maps a runtime operand layout to its compiled kernels.
+//
+// A layout code is L (one thread per number, L words) or (T << 16) | L (a
+// group of T lanes per number, L/T words per lane); see pg_limbs.h.
 #include "pg_limbs.h"
 #include "pg_search.cuh"
+#include "pg_search_group.cuh"
 
 namespace pg {
 
 #define PG_DECL(n) PG_DECLARE_LIMBS(n)
 PG_LIMB_LIST(PG_DECL)
 #undef PG_DECL
+#define PG_GDECL(t, lt) PG_GDECLARE(t, lt)
+PG_GROUP_LIST(PG_GDECL)
+#undef PG_GDECL
 
 bool supported_limbs(uint32_t L) {
 #define PG_CASE(n) \
     if (L == n) return true;
     PG_LIMB_LIST(PG_CASE)
 #undef PG_CASE
+#define PG_GCASE(t, lt) \
+    if (L == PG_LAYOUT_GROUP(t, (t) * (lt))) return true;
+    PG_GROUP_LIST(PG_GCASE)
+#undef PG_GCASE
     return false;
 }
 
-uint32_t pick_limbs(uint32_t words) {
+uint32_t pick_layout(uint32_t bits, uint32_t tpi) {
     uint32_t best = 0;
+    if (tpi <= 1) {
 #define PG_CASE(n) \
-    if (best == 0 && (uint32_t)n >= words) best = n;
-    PG_LIMB_LIST(PG_CASE)
+    if (best == 0 && 32u * (n) >= bits) best = n;
+        PG_LIMB_LIST(PG_CASE)
 #undef PG_CASE
+        if (best || tpi == 1) return best;
+    }
+    uint32_t bestL = 0;
+#define PG_GCASE(t, lt)                                                                                 \
+    if ((tpi == 0 || tpi == (uint32_t)(t)) && 32u * (t) * (lt) >= bits + 2 &&                           \
+        (bestL == 0 || (uint32_t)((t) * (lt)) < bestL)) {                                               \
+        bestL = (t) * (lt);                                                                             \
+        best = PG_LAYOUT_GROUP(t, (t) * (lt));                                                          \
+    }
+    PG_GROUP_LIST(PG_GCASE)
+#undef PG_GCASE
     return best;
 }
+
+uint32_t pick_limbs(uint32_t words) { return pick_layout(32 * words, 0); }
+
+uint32_t layout_words(uint32_t layout) { return layout & 0xffffu; }
 
 cudaError_t launch_prp_batch(uint32_t L, const uint32_t *cand, uint32_t words, uint32_t n, uint32_t rounds,
                              int32_t *out, cudaStream_t st) {
@@ -32,6 +59,10 @@ cudaError_t launch_prp_batch(uint32_t L, const uint32_t *cand, uint32_t words, u
     if (L == nl) return launch_prp_batch_t<nl>(cand, words, n, rounds, out, st);
     PG_LIMB_LIST(PG_CASE)
 #undef PG_CASE
+#define PG_GCASE(t, lt) \
+    if (L == PG_LAYOUT_GROUP(t, (t) * (lt))) return glaunch_prp_batch<t, lt>(cand, words, n, rounds, out, st);
+    PG_GROUP_LIST(PG_GCASE)
+#undef PG_GCASE
     return cudaErrorInvalidValue;
 }
 
@@ -42,6 +73,10 @@ int search_grid(uint32_t L, int device) {
     if (L == nl) per = search_occupancy_t<nl>();
     PG_LIMB_LIST(PG_CASE)
 #undef PG_CASE
+#define PG_GCASE(t, lt) \
+    if (L == PG_LAYOUT_GROUP(t, (t) * (lt))) per = gsearch_occupancy<t, lt>();
+    PG_GROUP_LIST(PG_GCASE)
+#undef PG_GCASE
     if (per < 1) per = 1;
     return sms * per;
 }
@@ -52,6 +87,10 @@ cudaError_t launch_search_persistent(uint32_t L, const SearchArgs &a, int grid, 
     if (L == nl) return launch_search_persistent_t<nl>(a, grid, st);
     PG_LIMB_LIST(PG_CASE)
 #undef PG_CASE
+#define PG_GCASE(t, lt) \
+    if (L == PG_LAYOUT_GROUP(t, (t) * (lt))) return glaunch_search_persistent<t, lt>(a, grid, st);
+    PG_GROUP_LIST(PG_GCASE)
+#undef PG_GCASE
     return cudaErrorInvalidValue;
 }
 
@@ -61,6 +100,10 @@ cudaError_t launch_search_plain(uint32_t L, const SearchArgs &a, uint32_t *k_nex
     if (L == nl) return launch_search_plain_t<nl>(a, k_next, st);
     PG_LIMB_LIST(PG_CASE)
 #undef PG_CASE
+#define PG_GCASE(t, lt) \
+    if (L == PG_LAYOUT_GROUP(t, (t) * (lt))) return glaunch_search_plain<t, lt>(a, k_next, st);
+    PG_GROUP_LIST(PG_GCASE)
+#undef PG_GCASE
     return cudaErrorInvalidValue;
 }
 
@@ -72,6 +115,11 @@ cudaError_t launch_finalize(uint32_t L, const SearchArgs &a, uint32_t nsides, ui
     if (L == nl) return launch_finalize_t<nl>(a, nsides, gaps, redo, n_redo, confirm_tests, k_start_rw, st);
     PG_LIMB_LIST(PG_CASE)
 #undef PG_CASE
+#define PG_GCASE(t, lt)                                                                                    \
+    if (L == PG_LAYOUT_GROUP(t, (t) * (lt)))                                                               \
+        return glaunch_finalize<t, lt>(a, nsides, gaps, redo, n_redo, confirm_tests, k_start_rw, st);
+    PG_GROUP_LIST(PG_GCASE)
+#undef PG_GCASE
     return cudaErrorInvalidValue;
 }
 

@@ -1,0 +1,294 @@
+// pg_group.cuh -- multi-precision Montgomery arithmetic with one number spread
+// over a group of T lanes (T in {4, 8, 16, 32}), LT words per lane, L = T*LT.
+//
+// For operands too wide for one thread's registers (P = 3001: 4 248-bit N,
+// 136 words).  Lane g of a group holds words [g*LT, (g+1)*LT) of every value.
+// Multiplication is CIOS, row by row: the row's word of `a` is broadcast by a
+// warp shuffle, every lane multiplies its slice, lane 0 of the group derives
+// the Montgomery factor q and broadcasts it, and the accumulator shifts down
+// one word by a shuffle.  A carry leaving a lane's slice is not passed on at
+// once: it waits as that lane's pending "spill" (it belongs to the next
+// lane's lowest word) and is folded in when the shift brings that word down,
+// so a row has no serial carry chain across lanes.  Carries that remain at
+// the end are resolved in one step by carry lookahead over warp ballots
+// (generate / propagate bits per lane, added as integers).
+//
+// Every shuffle and ballot names only the group's lanes, so the groups of a
+// warp may diverge (one idle, another still squaring).
+//
+// Values are kept in [0, 2n) ("almost Montgomery"): with 4n < R = 2^(32L),
+// a product of two values below 2n is again below 2n, so no conditional
+// subtraction is needed per multiplication.  Callers pick L with at least two
+// spare bits above the bit length of n.
+#pragma once
+
+#include <cstdint>
+
+#include "pg_mont.cuh"
+
+namespace pg {
+
+template <int T>
+struct Group {
+    static_assert(T == 2 || T == 4 || T == 8 || T == 16 || T == 32, "group size");
+    uint32_t lane, gl, gb;  // lane in warp, lane in group, first lane of the group
+    uint32_t gmask;         // the group's lanes as a bit mask
+    __device__ __forceinline__ Group() {
+        lane = threadIdx.x & 31;
+        gl = lane & (T - 1);
+        gb = lane - gl;
+        gmask = (T == 32) ? 0xffffffffu : (((1u << T) - 1) << gb);
+    }
+    // the group's T bits of a warp ballot, lane gb at bit 0
+    __device__ __forceinline__ uint32_t field(uint32_t ballot) const {
+        return (T == 32) ? ballot : ((ballot >> gb) & ((1u << T) - 1));
+    }
+};
+
+// Carry-in of this lane when every lane has a carry-out bit g (generate) and
+// a slice that would pass an incoming carry on (p, all ones): the carries of
+// a ripple through the group, found by adding (g|p) + g as T-bit integers.
+// Returns the lane's carry-in; *out receives the group's final carry-out.
+template <int T>
+__device__ __forceinline__ uint32_t lookahead(const Group<T> &G, bool g, bool p, uint32_t *out) {
+    const uint64_t gf = G.field(__ballot_sync(G.gmask, g));
+    const uint64_t pf = G.field(__ballot_sync(G.gmask, p));
+    const uint64_t a = gf | pf;
+    const uint64_t c = (a + gf) ^ a ^ gf;  // bit i = carry into lane i (bit T = out of the group)
+    if (out) *out = (uint32_t)((c >> T) & 1u);
+    return (uint32_t)((c >> G.gl) & 1u);
+}
+
+// x (slice) += cin (0 or 1) through the LT words
+template <int LT>
+__device__ __forceinline__ void slice_add_bit(uint32_t (&x)[LT], uint32_t cin) {
+    x[0] = add_cc(x[0], cin);
+#pragma unroll
+    for (int k = 1; k < LT; k++) x[k] = (k + 1 < LT) ? addc_cc(x[k], 0u) : addc(x[k], 0u);
+}
+
+// Adds the pending 64-bit value `in` (which belongs at this lane's lowest
+// word) and resolves all carries across the group.  Returns the group's final
+// carry-out (identical in every lane).
+template <int T, int LT>
+__device__ __forceinline__ uint32_t resolve_in(const Group<T> &G, uint32_t (&x)[LT], uint64_t in) {
+    static_assert(LT >= 2, "a lane holds at least two words");
+    x[0] = add_cc(x[0], (uint32_t)in);
+    if (LT > 1) {
+        x[1 < LT ? 1 : 0] = addc_cc(x[1 < LT ? 1 : 0], (uint32_t)(in >> 32));
+#pragma unroll
+        for (int k = 2; k < LT; k++) x[k] = addc_cc(x[k], 0u);
+    }
+    const uint32_t g = addc(0u, 0u) | (LT == 1 ? (uint32_t)(in >> 32) : 0u);
+    uint32_t all1 = 0xffffffffu;
+#pragma unroll
+    for (int k = 0; k < LT; k++) all1 &= x[k];
+    uint32_t out;
+    const uint32_t cin = lookahead<T>(G, g != 0, all1 == 0xffffffffu, &out);
+    slice_add_bit<LT>(x, cin);
+    return out;
+}
+
+// d = x - y across the group; returns 1 when x < y (a borrow leaves the top)
+template <int T, int LT>
+__device__ __forceinline__ uint32_t group_sub(const Group<T> &G, uint32_t (&d)[LT], const uint32_t (&x)[LT],
+                                              const uint32_t (&y)[LT]) {
+    d[0] = sub_cc(x[0], y[0]);
+#pragma unroll
+    for (int k = 1; k < LT; k++) d[k] = subc_cc(x[k], y[k]);
+    const uint32_t bout = subc(0u, 0u) & 1u;  // borrow out of the slice
+    uint32_t all0 = 0;
+#pragma unroll
+    for (int k = 0; k < LT; k++) all0 |= d[k];
+    uint32_t out;
+    const uint32_t bin = lookahead<T>(G, bout != 0, all0 == 0, &out);
+    // subtract the incoming borrow
+    d[0] = sub_cc(d[0], bin);
+#pragma unroll
+    for (int k = 1; k < LT; k++) d[k] = (k + 1 < LT) ? subc_cc(d[k], 0u) : subc(d[k], 0u);
+    return out;
+}
+
+template <int T, int LT>
+__device__ __forceinline__ bool group_eq(const uint32_t (&x)[LT], const uint32_t (&y)[LT]) {
+    uint32_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < LT; k++) acc |= x[k] ^ y[k];
+    const Group<T> G;
+    return G.field(__ballot_sync(G.gmask, acc != 0)) == 0;
+}
+
+// acc (slice) + spill += ai * b (slice): lo products chain over the slice, hi
+// products one word up; what leaves the slice is added to the spill.
+template <int LT>
+__device__ __forceinline__ void row_mac(uint32_t (&acc)[LT], uint64_t &spill, uint32_t ai, const uint32_t (&b)[LT]) {
+    acc[0] = mad_lo_cc(ai, b[0], acc[0]);
+#pragma unroll
+    for (int k = 1; k < LT; k++) acc[k] = madc_lo_cc(ai, b[k], acc[k]);
+    const uint32_t c1 = addc(0u, 0u);
+    uint32_t h;
+    if (LT > 1) {
+        acc[1 < LT ? 1 : 0] = mad_hi_cc(ai, b[0], acc[1 < LT ? 1 : 0]);
+#pragma unroll
+        for (int k = 1; k < LT - 1; k++) acc[k + 1] = madc_hi_cc(ai, b[k], acc[k + 1]);
+        h = madc_hi(ai, b[LT - 1], c1);
+    } else {
+        h = __umulhi(ai, b[0]) + c1;
+    }
+    spill += h;
+}
+
+// r = a * b * R^-1 mod n, inputs and output in [0, 2n), 4n < R
+template <int T, int LT>
+__device__ __forceinline__ void gmont_mul(const Group<T> &G, uint32_t (&r)[LT], const uint32_t (&a)[LT],
+                                          const uint32_t (&b)[LT], const uint32_t (&n)[LT], uint32_t ninv) {
+    uint32_t acc[LT];
+#pragma unroll
+    for (int k = 0; k < LT; k++) acc[k] = 0;
+    uint64_t spill = 0;
+    for (int src = 0; src < T; src++) {
+#pragma unroll
+        for (int w = 0; w < LT; w++) {
+            const uint32_t ai = __shfl_sync(G.gmask, a[w], G.gb + src);
+            row_mac<LT>(acc, spill, ai, b);
+            uint32_t q = acc[0] * ninv;  // meaningful in the group's lane 0
+            q = __shfl_sync(G.gmask, q, G.gb);
+            row_mac<LT>(acc, spill, q, n);
+            // shift down one word: this slice's lowest word is 0 in lane 0 and
+            // moves to the previous lane elsewhere; the next lane's lowest word
+            // (plus this lane's spill, which belongs to that position) arrives on top
+            uint32_t nxt = __shfl_down_sync(G.gmask, acc[0], 1);
+            if (G.gl == T - 1) nxt = 0;
+#pragma unroll
+            for (int k = 0; k < LT - 1; k++) acc[k] = acc[k + 1];
+            const uint64_t v = (uint64_t)nxt + spill;
+            acc[LT - 1] = (uint32_t)v;
+            spill = v >> 32;
+        }
+    }
+    // fold each spill into the next lane's lowest word and resolve the carries
+    const uint32_t lo = __shfl_up_sync(G.gmask, (uint32_t)spill, 1);
+    const uint32_t hi = __shfl_up_sync(G.gmask, (uint32_t)(spill >> 32), 1);
+    const uint64_t in = (G.gl == 0) ? 0ull : ((uint64_t)hi << 32 | lo);
+    resolve_in<T, LT>(G, acc, in);
+#pragma unroll
+    for (int k = 0; k < LT; k++) r[k] = acc[k];
+}
+
+// x = 2x mod 2n for x in [0, 2n): shift left one bit across the group, then
+// subtract 2n (n2) unless that borrows
+template <int T, int LT>
+__device__ __forceinline__ void gdbl(const Group<T> &G, uint32_t (&x)[LT], const uint32_t (&n2)[LT]) {
+    uint32_t y[LT];
+    const uint32_t topbit = x[LT - 1] >> 31;
+    uint32_t in = __shfl_up_sync(G.gmask, topbit, 1);
+    if (G.gl == 0) in = 0;
+#pragma unroll
+    for (int k = LT - 1; k >= 1; k--) y[k] = __funnelshift_l(x[k - 1], x[k], 1);
+    y[0] = (x[0] << 1) | in;
+    uint32_t d[LT];
+    const uint32_t borrow = group_sub<T, LT>(G, d, y, n2);
+#pragma unroll
+    for (int k = 0; k < LT; k++) x[k] = borrow ? y[k] : d[k];
+}
+
+// Strong probable-prime test of the odd group-held n (> base + 1) to `base`
+// (miller_rabin.h:216-248 for one base).  bits(n) <= 32*L - 2 is required.
+template <int T, int LT>
+__device__ __forceinline__ bool gstrong_prp(const Group<T> &G, const uint32_t (&n)[LT], uint32_t base) {
+    // ninv from the lowest word (lane 0), B and s = ctz(n-1) over the group
+    const uint32_t n0 = __shfl_sync(G.gmask, n[0], G.gb);
+    const uint32_t ninv = neg_inv32(n0);
+    int myB = 0, myS = 1 << 30;
+#pragma unroll
+    for (int k = 0; k < LT; k++) {
+        const int wi = G.gl * LT + k;
+        if (n[k]) myB = 32 * wi + 32 - __clz(n[k]);
+        const uint32_t w = (wi == 0) ? (n[k] & ~1u) : n[k];
+        if (w && myS == (1 << 30)) myS = 32 * wi + __ffs(w) - 1;
+    }
+#pragma unroll
+    for (int o = 1; o < T; o <<= 1) {
+        myB = max(myB, __shfl_xor_sync(G.gmask, myB, o));
+        myS = min(myS, __shfl_xor_sync(G.gmask, myS, o));
+    }
+    const int B = myB, s = myS;
+    // n2 = 2n
+    uint32_t n2[LT];
+    {
+        const uint32_t topbit = n[LT - 1] >> 31;
+        uint32_t in = __shfl_up_sync(G.gmask, topbit, 1);
+        if (G.gl == 0) in = 0;
+#pragma unroll
+        for (int k = LT - 1; k >= 1; k--) n2[k] = __funnelshift_l(n[k - 1], n[k], 1);
+        n2[0] = (n[0] << 1) | in;
+    }
+    // one = R mod 2n (a value below 2n congruent to R): 2^(B-1) doubled 32L - B + 1 times
+    uint32_t one[LT];
+    {
+        const int b = B - 1;
+#pragma unroll
+        for (int k = 0; k < LT; k++) one[k] = (G.gl * LT + k == (b >> 5)) ? (1u << (b & 31)) : 0u;
+        for (int i = 0; i < 32 * T * LT - B + 1; i++) gdbl<T, LT>(G, one, n2);
+    }
+    // x = Mont(base): base * R, by doubling (base 2) or repeated addition
+    uint32_t x[LT], bm[LT];
+#pragma unroll
+    for (int k = 0; k < LT; k++) x[k] = one[k];
+    if (base == 2) {
+        gdbl<T, LT>(G, x, n2);
+    } else {
+        for (uint32_t t = 1; t < base; t++) {  // x = x + one mod 2n
+            uint32_t y[LT];
+            y[0] = add_cc(x[0], one[0]);
+#pragma unroll
+            for (int k = 1; k < LT; k++) y[k] = addc_cc(x[k], one[k]);
+            const uint32_t c = addc(0u, 0u);  // belongs to the next lane's lowest word
+            const uint32_t cin = __shfl_up_sync(G.gmask, c, 1);
+            resolve_in<T, LT>(G, y, G.gl == 0 ? 0ull : (uint64_t)cin);
+            uint32_t d[LT];
+            const uint32_t borrow = group_sub<T, LT>(G, d, y, n2);
+#pragma unroll
+            for (int k = 0; k < LT; k++) x[k] = borrow ? y[k] : d[k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < LT; k++) bm[k] = x[k];
+    // exponent words (n with bit 0 cleared), read by a runtime bit index
+    uint32_t e[LT];
+#pragma unroll
+    for (int k = 0; k < LT; k++) e[k] = n[k];
+    uint32_t unit[LT];  // the plain number 1
+#pragma unroll
+    for (int k = 0; k < LT; k++) unit[k] = (G.gl == 0 && k == 0) ? 1u : 0u;
+    uint32_t nm1[LT];
+#pragma unroll
+    for (int k = 0; k < LT; k++) nm1[k] = (G.gl == 0 && k == 0) ? (n[0] & ~1u) : n[k];
+    for (int b = B - 2;; b--) {
+        if (b < s) {
+            uint32_t y[LT];
+            gmont_mul<T, LT>(G, y, x, unit, n, ninv);  // leave Montgomery form: y in [0, n]
+            const bool is1 = group_eq<T, LT>(y, unit);
+            const bool ism1 = group_eq<T, LT>(y, nm1);
+            if (ism1) return true;
+            if (is1) return b == s - 1;
+            if (b == 0) return false;
+        }
+        gmont_mul<T, LT>(G, x, x, x, n, ninv);
+        if (b >= s) {
+            const int w = b >> 5;
+            const uint32_t owner = (uint32_t)(w / LT);
+            const int idx = w - (int)(G.gl * LT);
+            const uint32_t mine = (idx >= 0 && idx < LT) ? e[idx] : 0u;
+            const uint32_t word = __shfl_sync(G.gmask, mine, G.gb + owner);
+            if ((word >> (b & 31)) & 1u) {
+                if (base == 2)
+                    gdbl<T, LT>(G, x, n2);
+                else
+                    gmont_mul<T, LT>(G, x, x, bm, n, ninv);
+            }
+        }
+    }
+}
+
+}  // namespace pg

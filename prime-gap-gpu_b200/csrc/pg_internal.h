@@ -122,6 +122,10 @@ cudaError_t launch_imad_peak(int grid, uint32_t iters, uint32_t *sink, cudaStrea
 void set_error(const char *msg);
 int search_grid(uint32_t L, int device);
 bool supported_limbs(uint32_t L);
-uint32_t pick_limbs(uint32_t words);  // smallest compiled L >= words, 0 if none
+uint32_t pick_limbs(uint32_t words);  // layout for operands of `words` words, 0 if none
+// layout for operands of `bits` bits: tpi 0 = automatic, 1 = one thread per
+// number, T = groups of T lanes; 0 if none is compiled
+uint32_t pick_layout(uint32_t bits, uint32_t tpi);
+uint32_t layout_words(uint32_t layout);  // total words of a layout
 
 }  // namespace pg

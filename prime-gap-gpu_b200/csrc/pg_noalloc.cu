@@ -165,7 +165,7 @@ extern "C" int pg_next_prime_noalloc(const uint32_t *d_numbers, uint32_t n, uint
     if (words == 0) return na_fail(PG_ERR_ARG, "words must be > 0");
     if (max_steps == 0) return na_fail(PG_ERR_ARG, "max_steps must be > 0");
     const uint32_t L = pick_limbs(words);
-    if (L == 0) return na_fail(PG_ERR_UNSUPPORTED, "words above the compiled limit of 48");
+    if (words > 48 || L == 0 || L > 48) return na_fail(PG_ERR_UNSUPPORTED, "words above the compiled limit of 48");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return na_fail(PG_ERR_CUDA, "cudaGetDevice", e);

@@ -10,7 +10,7 @@ pytestmark = pytest.mark.gpu
 
 
 def test_golden_vectors(ctx, prp_vectors):
-    items = [it for it in prp_vectors["items"] if it["bits"] <= 48 * 32]
+    items = prp_vectors["items"]
     nums = [int(it["n"], 16) for it in items]
     got1 = ctx.prp(nums, rounds=1)
     got4 = ctx.prp(nums, rounds=4)
@@ -53,6 +53,19 @@ def test_every_compiled_width(ctx, oracle):
             nums += [p, p * 3 if (p * 3).bit_length() <= bits else p + 2]
         got = ctx.prp(nums, rounds=1)
         assert list(got) == [oracle.prp(n, 1) for n in nums], words
+
+
+@pytest.mark.parametrize("e", [1279, 2203, 2281, 3217, 4253, 4423])
+def test_group_layouts_wide_numbers(ctx, oracle, e):
+    """Numbers above 48 words run on lane groups: Mersenne primes 2^e - 1 (all-ones
+    words stress every carry path), their neighbours, products and random odd numbers."""
+    rng = random.Random(e)
+    p = 2 ** e - 1
+    nums = [p, p - 2, p + 2, p * 3, p * 1_000_003, 2 ** e + 1]
+    nums += [rng.getrandbits(e) | (1 << (e - 1)) | 1 for _ in range(6)]
+    got = ctx.prp(nums, rounds=2)
+    assert list(got) == [oracle.prp(n, 2) for n in nums]
+    assert got[0] == 2
 
 
 def test_small_and_edge_numbers(ctx, oracle):

@@ -137,6 +137,30 @@ def test_slot_state_errors(pg):
         assert len(job.search(10_000_000, 1_000).ms) == pg.count_m(10_000_000, 1_000, 2310)
 
 
+@pytest.mark.parametrize("tpi", [4, 8])
+def test_group_layout_search_equals_single_thread(pg, tpi):
+    """The lane-group kernels (persistent, plain, confirmation) give the one-thread kernels' gaps."""
+    base = pg.Job(503, 2190, 10_000, 20_000_000, max_m_inc=6_000, max_m=2_000_000, rounds=2)
+    with base, pg.Job(503, 2190, 10_000, 20_000_000, max_m_inc=6_000, max_m=2_000_000, rounds=2, tpi=tpi) as grp:
+        assert grp.info["tpi"] == tpi and base.info["tpi"] == 1
+        want = base.search(1_000_000, 6_000)
+        for form in (pg.PG_SEARCH_PERSISTENT, pg.PG_SEARCH_PLAIN):
+            got = grp.search(1_000_000, 6_000, form)
+            assert np.array_equal(want.prev_gap, got.prev_gap) and np.array_equal(want.next_gap, got.next_gap)
+            assert got.stats["confirm_tests"] == want.stats["confirm_tests"]
+
+
+def test_cfg5_P3001_against_gmp(pg):
+    """P=3001, d=2190, X in [-40000, 40000], primes <= 1e10: 4 248-bit operands on 136-word lane groups."""
+    g = golden("gaps_cfg5.json")
+    with pg.Job(g["P"], g["d"], g["sl"], g["max_prime"], max_m_inc=64, max_m=g["m_start"] + g["m_inc"]) as job:
+        assert job.info["limbs"] == 136 and job.info["tpi"] == 8
+        for m, a, b in zip(g["ms"], g["prev_gap"], g["next_gap"]):
+            res = job.search(m, 1)
+            assert list(res.ms) == [m]
+            assert (int(res.prev_gap[0]), int(res.next_gap[0])) == (a, b), m
+
+
 def test_repeat_is_deterministic(pg):
     with pg.Job(337, 2310, 7_500, 1_000_000, max_m_inc=3_000, max_m=2 * 10**7) as job:
         a = job.search(10_000_000, 3_000)
