@@ -107,8 +107,9 @@ typedef struct {
                               0 = default (65536) */
     uint32_t ext_window;   /* extension positions past sl tried in the first pass; 0 = 64 */
     uint32_t flags;        /* PG_JOB_* */
-    uint32_t search_hits;  /* large primes expecting fewer hits per window than this are sieved
-                              by modular search, the others by stepping every X; 0 = 64 */
+    uint32_t search_hits;  /* 0 = every large prime above 2*sl+1 is sieved by modular search
+                              (default); n > 0 keeps primes expecting >= n hits per window on
+                              the kernel that steps every X */
     uint32_t tpi;          /* threads per number of the PRP kernels: 0 = automatic (one
                               thread up to 48 words, then groups), 1, or a group size 4 / 8 */
 } pg_job_params;

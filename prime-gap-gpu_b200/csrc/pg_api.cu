@@ -607,20 +607,26 @@ static int window_setup(pg_job *j, WinSlot &s, uint64_t m_start, uint64_t m_inc)
     return PG_OK;
 }
 
-// First prime-table index sieved by modular search rather than by stepping
-// every Y: primes whose expected hits in the window, nodd * (2 sly + 1) / p,
-// fall below search_hits (default 64; the measured crossover of the two
-// methods on the P=503 window is between 32 and 128).
-static uint64_t large_split(const pg_job *j, uint64_t nodd) {
-    if (j->np == 0) return 0;
-    if (j->prm.flags & PG_JOB_LARGE_STEP) return j->np;
-    if (j->prm.flags & PG_JOB_LARGE_SEARCH) return 0;
-    const double hits = j->prm.search_hits ? (double)j->prm.search_hits : 64.0;
-    const double pv = (double)nodd * (2.0 * j->sly + 1) / hits;
-    if (pv <= (double)j->seg_v0) return 0;
-    const double s = (pv - (double)j->seg_v0) / (double)j->seg_span;
+// prime-table index of the first segment starting at or above value v
+static uint64_t table_index_at(const pg_job *j, double v) {
+    if (v <= (double)j->seg_v0) return 0;
+    const double s = std::ceil((v - (double)j->seg_v0) / (double)j->seg_span);
     if (s >= (double)j->seg_off.size()) return j->np;
     return j->seg_off[(size_t)s];
+}
+
+// First prime-table index sieved by modular search rather than by stepping
+// every Y.  The search needs p > 2 sly + 1 (one hit per m); by default every
+// such prime is searched (with the hit walk, stepping is slower at any split
+// on the P=503 window); search_hits > 0 keeps primes expecting at least that
+// many hits, nodd * (2 sly + 1) / p, on the stepping kernel.
+static uint64_t large_split(const pg_job *j, uint64_t nodd) {
+    if (j->np == 0) return 0;
+    const uint64_t min_split = table_index_at(j, 2.0 * j->sly + 2);
+    if (j->prm.flags & PG_JOB_LARGE_STEP) return j->np;
+    if ((j->prm.flags & PG_JOB_LARGE_SEARCH) || j->prm.search_hits == 0) return min_split;
+    const double hits = (double)j->prm.search_hits;
+    return std::max(min_split, table_index_at(j, (double)nodd * (2.0 * j->sly + 1) / hits));
 }
 
 static int run_sieve(pg_job *j, WinSlot &s, bool compact) {

@@ -319,11 +319,27 @@ __device__ __forceinline__ uint64_t modsearch64(uint64_t A, uint64_t B, uint64_t
     return (uint64_t)x;
 }
 
-// One thread per prime p of [first, first + count).  With X = 2Y and the
-// odd m = m0 + 2j, p | m*K + X  <=>  u = Y + sly = (A*j + B) mod p with
-// A = -K mod p and B = sly - m0*K/2 mod p; every j of the window with
-// u <= 2*sly is a hit.  The next hit is found directly by modsearch, so a
-// prime costs O(log p) per hit instead of one step per Y.
+__device__ __forceinline__ uint64_t modsearch_any(uint64_t A, uint64_t B, uint64_t p, uint64_t W) {
+    if (p < (1ull << 32)) return modsearch32((uint32_t)A, (uint32_t)B, (uint32_t)p, (uint32_t)W);
+    return modsearch64(A, B, p, W);
+}
+
+__device__ __forceinline__ uint64_t mulmod_any(uint64_t a, uint64_t b, uint64_t p) {
+    if (p < (1ull << 32)) return (a * b) % p;
+    return (uint64_t)(((unsigned __int128)a * b) % p);
+}
+
+// One thread per prime p of [first, first + count), p > 2*sly + 1.  With
+// X = 2Y and the odd m = m0 + 2j, p | m*K + X  <=>  u = Y + sly =
+// (A*j + B) mod p with A = -K mod p and B = sly - m0*K/2 mod p; every j of the
+// window with u <= W = 2*sly is a hit (one per j, since p > W).
+// The first hit is found by modsearch in O(log p).  When more hits are
+// expected, the three-distance structure of the sequence gives every later
+// hit in O(1): with a = the first step whose shift A*a mod p = alpha lands
+// in [0, W] and b = the first step whose shift lands in [p-W, p) (i.e. -beta),
+// the hit after u is u + alpha (step a) if that is <= W, else u - beta (step
+// b) if u >= beta, else u + alpha - beta (step a + b).  Otherwise each next
+// hit is one more modsearch.
 template <typename T>
 __global__ void __launch_bounds__(256) k_sieve_large_search(const __grid_constant__ LargeArgs a, uint64_t first,
                                                             uint64_t count) {
@@ -339,17 +355,34 @@ __global__ void __launch_bounds__(256) k_sieve_large_search(const __grid_constan
     const uint64_t A = p - c;  // c in [1, p)
     uint64_t j = 0;
     while (j < a.nodd) {
-        uint64_t d, u;
-        if (p < (1ull << 32)) {
-            d = modsearch32((uint32_t)A, (uint32_t)B, (uint32_t)p, (uint32_t)W);
-            u = (A * d + B) % p;
-        } else {
-            d = modsearch64(A, B, p, W);
-            u = (uint64_t)(((unsigned __int128)A * d + B) % p);
-        }
+        const uint64_t d = modsearch_any(A, B, p, W);
+        uint64_t u = mulmod_any(A, d, p) + B;
+        if (u >= p) u -= p;
         j += d;
         if (j >= a.nodd) break;
-        for (uint64_t uu = u; uu <= W; uu += p) mark_hit(a, j, (uint32_t)uu);
+        mark_hit(a, j, (uint32_t)u);
+        if ((a.nodd - j - 1) * (W + 1) >= 2 * p) {  // two or more further hits expected: walk
+            const uint64_t sa = 1 + modsearch_any(A, A, p, W);
+            const uint64_t alpha = mulmod_any(A, sa, p);
+            const uint64_t aw = A + W >= p ? A + W - p : A + W;
+            const uint64_t sb = 1 + modsearch_any(A, aw, p, W - 1);
+            const uint64_t beta = p - mulmod_any(A, sb, p);
+            while (true) {
+                if (u + alpha <= W) {
+                    j += sa;
+                    u += alpha;
+                } else if (u >= beta) {
+                    j += sb;
+                    u -= beta;
+                } else {
+                    j += sa + sb;
+                    u = u + alpha - beta;
+                }
+                if (j >= a.nodd) break;
+                mark_hit(a, j, (uint32_t)u);
+            }
+            break;
+        }
         B = u + A >= p ? u + A - p : u + A;  // residue of j + 1
         j++;
     }
