@@ -117,6 +117,8 @@ typedef struct {
 /* large-prime sieve: 0 = automatic, else force one method */
 #define PG_JOB_LARGE_STEP   0x1u   /* step every X for every prime */
 #define PG_JOB_LARGE_SEARCH 0x2u   /* modular search for the next hit */
+#define PG_JOB_NO_GRAPH     0x4u   /* launch the persistent form's kernels one by one
+                                      instead of as one CUDA graph per window */
 
 typedef struct {
     uint32_t k_bits;          /* bits of K */
@@ -165,6 +167,8 @@ typedef struct {
     uint64_t kernel_launches; /* kernels of this library launched by the call */
     uint64_t h2d_bytes;       /* host-to-device bytes copied by the call */
     uint64_t d2h_bytes;       /* device-to-host bytes copied by the call */
+    uint32_t graph_launches;  /* CUDA graph launches (the persistent form's window is one graph) */
+    uint32_t pad;
 } pg_search_stats;
 
 /* Searches the window: for each m coprime to d (ascending; ms may be NULL)

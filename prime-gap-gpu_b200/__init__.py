@@ -39,6 +39,7 @@ PG_SEARCH_PLAIN = 1
 PG_MAX_WORDS = 160
 PG_JOB_LARGE_STEP = 0x1
 PG_JOB_LARGE_SEARCH = 0x2
+PG_JOB_NO_GRAPH = 0x4
 
 # every symbol include/primegap.h declares
 EXPORTS = (
@@ -84,6 +85,7 @@ class SearchStats(ctypes.Structure):
         ("sieve_ms", ctypes.c_double), ("prp_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
         ("search_kernel_ms", ctypes.c_double), ("kernel_launches", ctypes.c_uint64),
         ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
+        ("graph_launches", ctypes.c_uint32), ("pad", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:

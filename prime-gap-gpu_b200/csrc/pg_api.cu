@@ -49,6 +49,16 @@ extern "C" const char *pg_last_error(void) { return g_last_error.c_str(); }
 
 void pg::set_error(const char *msg) { g_last_error = msg; }
 
+// Timing events are recorded as external event nodes when the stream is
+// being captured, so they keep their timestamps inside a window's graph.
+static cudaError_t record_ev(cudaEvent_t e, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t err = cudaStreamIsCapturing(st, &cs);
+    if (err != cudaSuccess) return err;
+    return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(e, st, cudaEventRecordExternal)
+                                               : cudaEventRecord(e, st);
+}
+
 extern "C" const char *pg_version(void) { return "primegap-b200 0.2 (sm_100a)"; }
 
 // ======================================================= host bignum (K)
@@ -157,6 +167,7 @@ struct WinSlot {
     int32_t *h_rank = nullptr;  // pinned
     uint32_t *h_gaps = nullptr; // pinned
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaGraphExec_t gexec = nullptr;  // the persistent form's window graph
     // in-flight state
     bool busy = false;
     uint64_t ticket = 0;
@@ -332,6 +343,7 @@ static void slot_free(WinSlot &s) {
     cudaFreeHost(s.h_gaps);
     for (auto &e : s.ev)
         if (e) cudaEventDestroy(e);
+    if (s.gexec) cudaGraphExecDestroy(s.gexec);
     if (s.st) cudaStreamDestroy(s.st);
 }
 
@@ -579,8 +591,8 @@ extern "C" void *pg_job_stream(pg_job *j, int slot) {
 // ============================================================== windows
 
 // Computes the coprime m and the odd-m rank table of a window into the
-// slot's pinned staging and uploads them on the slot's stream.
-static int window_setup(pg_job *j, WinSlot &s, uint64_t m_start, uint64_t m_inc) {
+// slot's pinned staging (host work only).
+static int window_tables(pg_job *j, WinSlot &s, uint64_t m_start, uint64_t m_inc) {
     const pg_job_params &p = j->prm;
     if (m_inc == 0) return fail(PG_ERR_ARG, "m_inc must be > 0");
     if (m_inc > std::max<uint64_t>(p.max_m_inc, 2))
@@ -602,9 +614,19 @@ static int window_setup(pg_job *j, WinSlot &s, uint64_t m_start, uint64_t m_inc)
         }
     }
     s.nm = r;
-    if (r) PG_CUDA(cudaMemcpyAsync(s.d_ms, s.h_ms, (size_t)r * 8, cudaMemcpyHostToDevice, s.st));
+    return PG_OK;
+}
+
+// Uploads the window tables on the slot's stream.
+static int window_upload(WinSlot &s) {
+    if (s.nm) PG_CUDA(cudaMemcpyAsync(s.d_ms, s.h_ms, (size_t)s.nm * 8, cudaMemcpyHostToDevice, s.st));
     if (s.nodd) PG_CUDA(cudaMemcpyAsync(s.d_rank, s.h_rank, (size_t)s.nodd * 4, cudaMemcpyHostToDevice, s.st));
     return PG_OK;
+}
+
+static int window_setup(pg_job *j, WinSlot &s, uint64_t m_start, uint64_t m_inc) {
+    int rc = window_tables(j, s, m_start, m_inc);
+    return rc ? rc : window_upload(s);
 }
 
 // prime-table index of the first segment starting at or above value v
@@ -720,11 +742,13 @@ static int enqueue_finalize(pg_job *j, WinSlot &s, SearchArgs &a, uint32_t S) {
     PG_CUDA(cudaMemsetAsync(&s.d_sc->n_redo, 0, 4, s.st));
     PG_CUDA(launch_finalize(j->L, a, S, s.d_gaps, s.d_redo, &s.d_sc->n_redo, &s.d_sc->confirm, s.d_kstart, s.st));
     s.sst.kernel_launches++;
-    PG_CUDA(cudaEventRecord(s.ev[2], s.st));  // end of the device work (before the copies back)
+    PG_CUDA(record_ev(s.ev[2], s.st));  // end of the device work (before the copies back)
     PG_CUDA(cudaMemcpyAsync(s.h_gaps, s.d_gaps, (size_t)S * 4, cudaMemcpyDeviceToHost, s.st));
     PG_CUDA(cudaMemcpyAsync(s.h_sc, s.d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s.st));
     return PG_OK;
 }
+
+static int enqueue_window(pg_job *j, WinSlot &s, int form, uint32_t flags);
 
 extern "C" int pg_search_submit(pg_job *j, uint64_t m_start, uint64_t m_inc, int form, uint32_t flags,
                                 uint64_t *ticket) {
@@ -737,17 +761,52 @@ extern "C" int pg_search_submit(pg_job *j, uint64_t m_start, uint64_t m_inc, int
     if (rc) return rc;
     PG_CUDA(cudaStreamSynchronize(s.st));  // the slot's pinned staging is reused
     s.sst = pg_search_stats{};
-    if ((rc = window_setup(j, s, m_start, m_inc))) return rc;
+    if ((rc = window_tables(j, s, m_start, m_inc))) return rc;
     s.sst.m_count = s.nm;
     s.sst.h2d_bytes = (uint64_t)s.nm * 8 + (uint64_t)s.nodd * 4;
     s.ticket = j->next_ticket++;
     s.busy = true;
     *ticket = s.ticket;
     if (s.nm == 0) return PG_OK;
+    if (form == PG_SEARCH_PLAIN || (j->prm.flags & PG_JOB_NO_GRAPH)) return enqueue_window(j, s, form, flags);
+    // The persistent form's whole window (upload, sieves, search, finalize,
+    // copies back) is captured as one CUDA graph and launched once; the slot
+    // keeps the instantiated graph and updates it in place for the next window.
+    PG_CUDA(cudaStreamBeginCapture(s.st, cudaStreamCaptureModeThreadLocal));
+    rc = enqueue_window(j, s, form, flags);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(s.st, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (ec != cudaSuccess) return fail(PG_ERR_CUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(ec));
+    if (s.gexec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(s.gexec, g, &info) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(s.gexec);
+            s.gexec = nullptr;
+        }
+    }
+    cudaError_t ei = cudaSuccess;
+    if (!s.gexec) ei = cudaGraphInstantiate(&s.gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return fail(PG_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(ei));
+    PG_CUDA(cudaGraphLaunch(s.gexec, s.st));
+    s.sst.graph_launches = 1;
+    return PG_OK;
+}
+
+// Enqueues one window's device work on the slot's stream (capturable for the
+// persistent form; the plain form reads counts back and is not).
+static int enqueue_window(pg_job *j, WinSlot &s, int form, uint32_t flags) {
+    int rc;
     const uint32_t S = 2 * s.nm;
-    PG_CUDA(cudaEventRecord(s.ev[0], s.st));
+    if ((rc = window_upload(s))) return rc;
+    PG_CUDA(record_ev(s.ev[0], s.st));
     if ((rc = run_sieve(j, s, true))) return rc;
-    PG_CUDA(cudaEventRecord(s.ev[1], s.st));
+    PG_CUDA(record_ev(s.ev[1], s.st));
     const uint32_t warps = (uint32_t)j->grid * 4;
     PG_CUDA(launch_init_search(S, s.d_found, s.d_kstart, s.d_act0, s.d_sc, warps, s.st));
     s.sst.kernel_launches++;
@@ -764,16 +823,16 @@ extern "C" int pg_search_submit(pg_job *j, uint64_t m_start, uint64_t m_inc, int
             a.drain_lanes = 4;
             a.min_warps = (uint32_t)j->ctx->sms;
         }
-        PG_CUDA(cudaEventRecord(s.ev[3], s.st));
+        PG_CUDA(record_ev(s.ev[3], s.st));
         PG_CUDA(launch_search_persistent(j->L, a, j->grid, s.st));
-        PG_CUDA(cudaEventRecord(s.ev[4], s.st));
+        PG_CUDA(record_ev(s.ev[4], s.st));
         s.sst.kernel_launches++;
         s.sst.passes = 1;
     } else {  // one launch per pass, the active-side count read back after each
         PG_CUDA(cudaMemsetAsync(s.d_knext, 0, (size_t)S * 4, s.st));
         uint32_t n_act = S;
         uint32_t *cur = s.d_act0, *nxt = s.d_act1;
-        PG_CUDA(cudaEventRecord(s.ev[3], s.st));
+        PG_CUDA(record_ev(s.ev[3], s.st));
         while (n_act > 0) {
             a.act = cur;
             a.n_act = n_act;
@@ -789,7 +848,7 @@ extern "C" int pg_search_submit(pg_job *j, uint64_t m_start, uint64_t m_inc, int
             n_act = s.h_sc->n_out;
             std::swap(cur, nxt);
         }
-        PG_CUDA(cudaEventRecord(s.ev[4], s.st));
+        PG_CUDA(record_ev(s.ev[4], s.st));
         PG_CUDA(launch_iota(s.d_act0, S, s.st));
         s.sst.kernel_launches++;
     }
@@ -828,7 +887,7 @@ static int slot_finish(pg_job *j, WinSlot &s) {
         PG_CUDA(cudaMemsetAsync(&s.d_sc->n_redo, 0, 4, s.st));
         PG_CUDA(launch_finalize(j->L, a, S, s.d_gaps, s.d_redo, &s.d_sc->n_redo, &s.d_sc->confirm, s.d_kstart, s.st));
         s.sst.kernel_launches++;
-        PG_CUDA(cudaEventRecord(s.ev[2], s.st));
+        PG_CUDA(record_ev(s.ev[2], s.st));
         PG_CUDA(cudaMemcpyAsync(s.h_gaps, s.d_gaps, (size_t)S * 4, cudaMemcpyDeviceToHost, s.st));
         PG_CUDA(cudaMemcpyAsync(s.h_sc, s.d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s.st));
         s.sst.d2h_bytes += 4;
@@ -858,9 +917,10 @@ extern "C" int pg_search_wait(pg_job *j, uint64_t ticket, uint64_t *ms, uint32_t
     if (ms) std::memcpy(ms, s.h_ms, (size_t)s.nm * 8);
     s.sst.d2h_bytes += (uint64_t)2 * s.nm * 4 + sizeof(Scalars);
     float t_sieve = 0, t_prp = 0, t_kernel = 0;
-    cudaEventElapsedTime(&t_sieve, s.ev[0], s.ev[1]);
-    cudaEventElapsedTime(&t_prp, s.ev[1], s.ev[2]);
-    cudaEventElapsedTime(&t_kernel, s.ev[3], s.ev[4]);
+    if (cudaEventElapsedTime(&t_sieve, s.ev[0], s.ev[1]) != cudaSuccess) t_sieve = 0;
+    if (cudaEventElapsedTime(&t_prp, s.ev[1], s.ev[2]) != cudaSuccess) t_prp = 0;
+    if (cudaEventElapsedTime(&t_kernel, s.ev[3], s.ev[4]) != cudaSuccess) t_kernel = 0;
+    cudaGetLastError();  // a failed timing read must not surface in a later call
     s.sst.search_kernel_ms = t_kernel;
     s.sst.sieve_ms = t_sieve;
     s.sst.prp_ms = t_prp;

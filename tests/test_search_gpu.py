@@ -161,6 +161,20 @@ def test_cfg5_P3001_against_gmp(pg):
             assert (int(res.prev_gap[0]), int(res.next_gap[0])) == (a, b), m
 
 
+def test_graph_and_direct_launches_agree(pg):
+    """The persistent form runs each window as one CUDA graph (updated in place for the next
+    window); with PG_JOB_NO_GRAPH the same kernels are launched one by one."""
+    windows = [(10_000_000, 3_000), (10_003_000, 3_000), (10_006_000, 1_999), (10_000_000, 3_000)]
+    kw = dict(max_m_inc=3_000, max_m=2 * 10**7)
+    with pg.Job(337, 2310, 7_500, 2_000_000, **kw) as g, \
+            pg.Job(337, 2310, 7_500, 2_000_000, flags=pg.PG_JOB_NO_GRAPH, **kw) as d:
+        for a, b in windows:
+            rg, rd = g.search(a, b), d.search(a, b)
+            assert rg.stats["graph_launches"] == 1 and rd.stats["graph_launches"] == 0
+            assert np.array_equal(rg.prev_gap, rd.prev_gap) and np.array_equal(rg.next_gap, rd.next_gap)
+            assert rg.stats["prp_ms"] > 0 and rg.stats["sieve_ms"] > 0
+
+
 def test_repeat_is_deterministic(pg):
     with pg.Job(337, 2310, 7_500, 1_000_000, max_m_inc=3_000, max_m=2 * 10**7) as job:
         a = job.search(10_000_000, 3_000)
