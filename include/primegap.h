@@ -228,6 +228,16 @@ int pg_search_wait(pg_job *job, uint64_t ticket, uint64_t *ms, uint32_t *prev_ga
 /* cudaStream_t of window slot `slot` (for CUDA-event timing by callers). */
 void *pg_job_stream(pg_job *job, int slot);
 
+/* Autotuner (no counterpart in the reference, which fixes these at compile
+ * time, gpu_testing.cu:44-62).  Starting from *base, times searches of the
+ * sample window [m_start, m_start + m_inc) and writes to *best the fastest
+ * small_limit (the prime bound of the per-m shared-memory sieve tile, tried
+ * 16384 / 65536 / 262144) and then threads per number (tpi 1, 4, 8 where a
+ * compiled layout fits the operand width; the limb count follows), and to
+ * *best_ms its device time per window.  Builds one job per candidate. */
+int pg_autotune(pg_ctx *ctx, const pg_job_params *base, uint64_t m_start, uint64_t m_inc, pg_job_params *best,
+                double *best_ms);
+
 /* Merit of a gap as overflow.cpp:162: gap / (k_log + log(m)). */
 double pg_merit(double k_log, uint64_t m, uint64_t gap);
 

@@ -47,7 +47,7 @@ EXPORTS = (
     "pg_prp_batch", "pg_prp_batch_device",
     "pg_job_create", "pg_job_destroy", "pg_job_get_info", "pg_job_k_words",
     "pg_count_m", "pg_sieve_interval", "pg_search", "pg_merit", "pg_format_record", "pg_next_prime_noalloc",
-    "pg_search_submit", "pg_search_wait", "pg_job_stream",
+    "pg_search_submit", "pg_search_wait", "pg_job_stream", "pg_autotune",
 )
 PG_SEARCH_SLOTS = 2
 PG_SUBMIT_DRAIN = 0x1
@@ -123,6 +123,8 @@ def _load() -> ctypes.CDLL:
     lib.pg_search_wait.argtypes = [vp, u64, P64, P32, P32, ctypes.POINTER(SearchStats)]
     lib.pg_job_stream.restype = vp
     lib.pg_job_stream.argtypes = [vp, i32]
+    lib.pg_autotune.argtypes = [vp, ctypes.POINTER(JobParams), u64, u64, ctypes.POINTER(JobParams),
+                                ctypes.POINTER(ctypes.c_double)]
     lib.pg_merit.restype = ctypes.c_double
     lib.pg_merit.argtypes = [ctypes.c_double, u64, u64]
     lib.pg_format_record.argtypes = [ctypes.c_char_p, ctypes.c_size_t, u64, ctypes.c_double, u64, u32, u32, u64]
@@ -351,6 +353,37 @@ class Job:
             if mer > min_merit:
                 out.append(format_record(pg + ng, mer, m, self.p, self.d, pg))
         return out
+
+
+JOB_KNOBS = ("rounds", "small_limit", "ext_window", "flags", "search_hits", "tpi")
+
+
+def autotune(p: int, d: int, sl: int, max_prime: int, m_start: int, m_inc: int, ctx: Context | None = None,
+             cache: str | pathlib.Path | None = None, **knobs) -> tuple[dict, float]:
+    """Times the sample window [m_start, m_start + m_inc) with candidate sieve
+    tiles and operand layouts (pg_autotune) and returns (best knobs, ms per
+    window).  With `cache`, results are kept in that JSON file, keyed by the
+    job's shape and the operand bit length, and reused."""
+    import json
+    key = None
+    if cache is not None:
+        cache = pathlib.Path(cache)
+        store = json.loads(cache.read_text()) if cache.exists() else {}
+        key = f"P{p}/d{d}/sl{sl}/limit{max_prime}/minc{m_inc}/m{m_start.bit_length()}bits/" + \
+              "/".join(f"{k}={knobs[k]}" for k in sorted(knobs))
+        if key in store:
+            return store[key]["knobs"], store[key]["ms"]
+    ctx = ctx or Context(0)
+    base = JobParams(p, d, sl, max_prime, m_inc, m_start + m_inc, knobs.get("rounds", 1), knobs.get("small_limit", 0),
+                     knobs.get("ext_window", 0), knobs.get("flags", 0), knobs.get("search_hits", 0), knobs.get("tpi", 0))
+    best = JobParams()
+    ms = ctypes.c_double(0)
+    _check(lib.pg_autotune(ctx.handle, ctypes.byref(base), m_start, m_inc, ctypes.byref(best), ctypes.byref(ms)))
+    out = {k: getattr(best, k) for k in JOB_KNOBS}
+    if key is not None:
+        store[key] = {"knobs": out, "ms": ms.value}
+        cache.write_text(json.dumps(store, indent=1))
+    return out, ms.value
 
 
 def merit(k_log: float, m: int, gap: int) -> float:

@@ -939,6 +939,69 @@ extern "C" int pg_search(pg_job *j, uint64_t m_start, uint64_t m_inc, int form, 
     return pg_search_wait(j, t, ms, prev_gap, next_gap, stats);
 }
 
+// ============================================================ autotune
+
+// device time of one search of the window with params p (a warm-up search first)
+static int time_params(pg_ctx *c, const pg_job_params &p, uint64_t m_start, uint64_t m_inc, double *ms) {
+    pg_job *j = nullptr;
+    int rc = pg_job_create(c, &p, &j);
+    if (rc) return rc;
+    pg_search_stats st{};
+    double best = 1e300;
+    for (int rep = 0; rep < 3 && rc == PG_OK; rep++) {
+        rc = pg_search(j, m_start, m_inc, PG_SEARCH_PERSISTENT, nullptr, nullptr, nullptr, &st);
+        if (rep > 0) best = std::min(best, st.total_ms);
+    }
+    pg_job_destroy(j);
+    *ms = best;
+    return rc;
+}
+
+extern "C" int pg_autotune(pg_ctx *c, const pg_job_params *base, uint64_t m_start, uint64_t m_inc, pg_job_params *best,
+                           double *best_ms) {
+    if (!c || !base || !best) return fail(PG_ERR_ARG, "pg_autotune: NULL argument");
+    pg_job_params p = *base;
+    p.max_m_inc = std::max<uint64_t>(p.max_m_inc, m_inc);
+    p.max_m = std::max<uint64_t>(p.max_m, m_start + m_inc);
+    double top = 1e300;
+    pg_job_params winner = p;
+    // 1. the shared-memory sieve's prime bound
+    const uint32_t smalls[] = {16384, 65536, 262144};
+    for (uint32_t v : smalls) {
+        if (v > p.max_prime && v != smalls[0]) continue;
+        pg_job_params q = p;
+        q.small_limit = v;
+        double ms = 0;
+        int rc = time_params(c, q, m_start, m_inc, &ms);
+        if (rc == PG_ERR_UNSUPPORTED) continue;
+        if (rc) return rc;
+        if (ms < top) {
+            top = ms;
+            winner = q;
+        }
+    }
+    // 2. threads per number (the operand layout)
+    const uint32_t tpis[] = {1, 4, 8};
+    const uint32_t keep_tpi = winner.tpi;
+    for (uint32_t t : tpis) {
+        pg_job_params q = winner;
+        q.tpi = t;
+        if (t == keep_tpi) continue;
+        double ms = 0;
+        int rc = time_params(c, q, m_start, m_inc, &ms);
+        if (rc == PG_ERR_UNSUPPORTED) continue;  // no layout of that width fits
+        if (rc) return rc;
+        if (ms < top) {
+            top = ms;
+            winner = q;
+        }
+    }
+    g_last_error.clear();
+    *best = winner;
+    if (best_ms) *best_ms = top;
+    return PG_OK;
+}
+
 // ============================================================= records
 
 extern "C" double pg_merit(double k_log, uint64_t m, uint64_t gap) { return (double)gap / (k_log + std::log((double)m)); }

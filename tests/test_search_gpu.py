@@ -175,6 +175,19 @@ def test_graph_and_direct_launches_agree(pg):
             assert rg.stats["prp_ms"] > 0 and rg.stats["sieve_ms"] > 0
 
 
+def test_autotune_picks_a_valid_faster_setting(pg, tmp_path):
+    cache = tmp_path / "tune.json"
+    knobs, ms = pg.autotune(337, 2310, 2_000, 5_000_000, 10_000_000, 2_000, cache=cache)
+    assert ms > 0 and knobs["small_limit"] in (16384, 65536, 262144) and knobs["tpi"] in (0, 1, 4, 8)
+    assert cache.exists()
+    again, ms2 = pg.autotune(337, 2310, 2_000, 5_000_000, 10_000_000, 2_000, cache=cache)
+    assert again == knobs and ms2 == ms  # served from the cache
+    with pg.Job(337, 2310, 2_000, 5_000_000, max_m_inc=2_000, max_m=2 * 10**7, **knobs) as tuned, \
+            pg.Job(337, 2310, 2_000, 5_000_000, max_m_inc=2_000, max_m=2 * 10**7) as plain:
+        a, b = tuned.search(10_000_000, 2_000), plain.search(10_000_000, 2_000)
+    assert np.array_equal(a.prev_gap, b.prev_gap) and np.array_equal(a.next_gap, b.next_gap)
+
+
 def test_repeat_is_deterministic(pg):
     with pg.Job(337, 2310, 7_500, 1_000_000, max_m_inc=3_000, max_m=2 * 10**7) as job:
         a = job.search(10_000_000, 3_000)
