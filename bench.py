@@ -337,6 +337,99 @@ def run_reference(args) -> dict:
             "prp_tests_per_sec": last["prp_tests_per_sec"]}
 
 
+# ----------------------------------------------------------- serving
+
+SERVE_SEED = 4
+
+
+def serve_requests(n: int = 256, seed: int = SERVE_SEED, limit: int = 1_000_000_000) -> list[tuple]:
+    """The serving mix: n requests, P in {337, 503, 907}, d in {210, 2190,
+    2310}, windows of 500-20,000 m starting uniformly in [1e6, 1e9],
+    SL = round(8 ln N) with N = m_start * P#/d, sieve limit 1e9."""
+    import numpy as np
+    import __graft_entry__
+    pg = __graft_entry__.load_package()
+    rng = np.random.default_rng(seed)
+    primorial = {}
+    for P in (337, 503, 907):
+        k = 1
+        for q in range(2, P + 1):
+            if all(q % r for r in range(2, int(q ** 0.5) + 1)):
+                k *= q
+        primorial[P] = k
+    out = []
+    for _ in range(n):
+        P = int(rng.choice([337, 503, 907]))
+        d = int(rng.choice([210, 2190, 2310]))
+        inc = int(rng.integers(500, 20_001))
+        start = int(rng.integers(1_000_000, 1_000_000_001))
+        sl = round(8 * (pg.k_log_of(primorial[P] // d) + math.log(start)))
+        out.append((P, d, sl, limit, start, inc))
+    return out
+
+
+def run_serve(args) -> dict:
+    """Capacity (all requests queued at once) and latency under Poisson
+    arrivals at 70% of that capacity, through pg_server_*."""
+    import threading
+    import numpy as np
+    import __graft_entry__
+    pg = __graft_entry__.load_package()
+    reqs = serve_requests(args.serve_jobs)
+    classes = sorted({(p, d) for p, d, *_ in reqs})
+    max_sl = max(r[2] for r in reqs)
+    with pg.Server(0, max_sl=max_sl) as srv:
+        # resident tables for every (P, d) first: one small request per class
+        warm = [srv.submit(p, d, 1_000, reqs[0][3], 1_000_001, 200) for p, d in classes]
+        t = time.perf_counter()
+        for i in warm:
+            srv.wait(i)
+        table_s = time.perf_counter() - t
+        # closed loop: every request at once
+        t0 = srv.clock()
+        ids = [srv.submit(p, d, sl, lim, m0, inc) for p, d, sl, lim, m0, inc in reqs]
+        infos = [srv.wait(i).info for i in ids]
+        span = max(x["done_s"] for x in infos) - t0
+        m_total = sum(x["m_count"] for x in infos)
+        cap_jobs = len(reqs) / span
+        st_closed = srv.stats()
+        # open loop: Poisson arrivals at 70% of capacity
+        rate = 0.7 * cap_jobs
+        gaps = np.random.default_rng(SERVE_SEED + 1).exponential(1.0 / rate, len(reqs))
+        arrivals = np.cumsum(gaps)
+        ids2 = [None] * len(reqs)
+
+        def feeder():
+            base = time.perf_counter()
+            for k, r in enumerate(reqs):
+                delay = arrivals[k] - (time.perf_counter() - base)
+                if delay > 0:
+                    time.sleep(delay)
+                ids2[k] = srv.submit(*r)
+
+        th = threading.Thread(target=feeder)
+        th.start()
+        th.join()
+        lat = np.array([(lambda x: x["done_s"] - x["submit_s"])(srv.wait(i).info) for i in ids2]) * 1e3
+        st = srv.stats()
+    return {
+        "metric": "serving latency p99 (256 gap-search requests, Poisson arrivals at 70% of capacity)",
+        "value": round(float(np.percentile(lat, 99)), 2), "unit": "ms", "higher_is_better": False,
+        "p50_ms": round(float(np.percentile(lat, 50)), 2), "p99_ms": round(float(np.percentile(lat, 99)), 2),
+        "mean_ms": round(float(lat.mean()), 2),
+        "capacity_jobs_per_s": round(cap_jobs, 2), "capacity_m_per_s": round(m_total / span, 1),
+        "arrival_rate_jobs_per_s": round(rate, 2), "closed_loop_s": round(span, 3),
+        "table_build_s": round(table_s, 3),
+        "launches": st_closed["launches"], "windows": st_closed["windows"],
+        "prp_tests_closed": st_closed["prp_tests"], "sieve_ms_closed": round(st_closed["sieve_ms"], 1),
+        "prp_ms_closed": round(st_closed["prp_ms"], 1), "peak_bytes": st["peak_bytes"],
+        "n_gpus": 1, "data": "synthetic (seeded request mix)",
+        "config": {"workload": f"{len(reqs)} requests, P in {{337,503,907}}, d in {{210,2190,2310}}, "
+                               "500-20000 m from [1e6,1e9], SL=round(8 ln N), primes <= 1e9",
+                   "seed": SERVE_SEED},
+    }
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -349,7 +442,13 @@ def main(argv=None) -> int:
                     help="let the PRP kernel's warps leave as a window drains (PG_SUBMIT_DRAIN)")
     ap.add_argument("--m-inc", type=int, default=WORKLOAD["m_inc"],
                     help="m per window (default 200000; smaller windows are for profiling only)")
+    ap.add_argument("--serve", action="store_true",
+                    help="the serving workload instead: p50/p99 latency of a request mix (pg_server_*)")
+    ap.add_argument("--serve-jobs", type=int, default=256)
     args = ap.parse_args(argv)
+    if args.serve:
+        print(json.dumps(run_serve(args)), flush=True)
+        return 0
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -238,6 +238,88 @@ void *pg_job_stream(pg_job *job, int slot);
 int pg_autotune(pg_ctx *ctx, const pg_job_params *base, uint64_t m_start, uint64_t m_inc, pg_job_params *best,
                 double *best_ms);
 
+/* ---------------------------------------------------------------- serving
+ *
+ * A server takes gap-search requests (any P, d, sl, sieve limit and m range)
+ * from any host thread and runs them on one device with continuous batching:
+ * a worker thread cuts each request's m range into windows, and packs windows
+ * of every admitted request whose operands share a layout into one search
+ * launch (one persistent PRP kernel over all their sides), two launches in
+ * flight.  Prime tables depend on (P, d, max_prime, small_limit) only and are
+ * shared by every request with that key, whatever its sl or m range.  A
+ * request is admitted once its tables are resident; tables that would not fit
+ * the device-memory budget wait until idle tables can be evicted (least
+ * recently used first).  The reference runs one (P, d, sl, range) per process
+ * (gap_search_gpu.cpp:106-135) and has no counterpart. */
+typedef struct pg_server pg_server;
+
+typedef struct {
+    uint64_t hbm_budget;   /* device bytes for tables and batch buffers; 0 = 3/4 of the free memory */
+    uint32_t batch_m;      /* coprime m per search launch (all its windows); 0 = 65536 */
+    uint32_t window_m;     /* requests are cut into windows of at most this many m; 0 = 65536 */
+    uint32_t max_windows;  /* windows per search launch; 0 = 64 */
+    uint32_t max_sl;       /* largest sl accepted; 0 = 20000 */
+    uint32_t small_limit;  /* as pg_job_params (0 = default) */
+    uint32_t ext_window;   /* as pg_job_params (0 = default) */
+    uint32_t tpi;          /* as pg_job_params (0 = automatic) */
+    uint32_t pad;
+} pg_server_params;
+
+typedef struct {
+    uint32_t p, d, sl;     /* as pg_job_params */
+    uint32_t rounds;       /* as pg_job_params (0 = 1) */
+    uint64_t max_prime;    /* sieve limit */
+    uint64_t m_start;      /* the m range [m_start, m_start + m_inc) */
+    uint64_t m_inc;
+} pg_request;
+
+typedef struct {
+    uint64_t m_count;      /* m searched: pg_count_m(m_start, m_inc, d) */
+    double k_log;          /* log(K) of the request's K = P#/d */
+    double submit_s;       /* server clock (seconds since pg_server_create): submitted */
+    double start_s;        /* first window launched */
+    double done_s;         /* last window finished */
+    uint32_t windows;      /* windows the range was cut into */
+    int32_t status;        /* PG_OK, or the error that failed the request */
+} pg_request_info;
+
+typedef struct {
+    uint64_t requests_done;  /* completed (or failed) requests */
+    uint64_t m_done;         /* m searched */
+    uint64_t prp_tests;      /* strong base-2 tests */
+    uint64_t launches;       /* search launches (batches) */
+    uint64_t windows;        /* windows run */
+    uint64_t tables_built;   /* prime-table builds */
+    uint64_t tables_evicted; /* prime tables dropped to admit others */
+    uint64_t resident_bytes; /* device bytes held now */
+    uint64_t peak_bytes;     /* most device bytes held */
+    double sieve_ms;         /* device time of the sieves, summed over launches */
+    double prp_ms;           /* device time of the searches, summed over launches */
+    double busy_s;           /* wall time with at least one launch in flight */
+} pg_server_stats;
+
+/* Starts a server (and its worker thread) on CUDA device `device`. */
+int pg_server_create(int device, const pg_server_params *params, pg_server **out);
+/* Queues a request and returns at once with its id.  Argument errors are
+ * returned here; errors found later (d does not divide P#, tables larger than
+ * the budget, CUDA errors) fail the request and come back from wait. */
+int pg_server_submit(pg_server *srv, const pg_request *rq, uint64_t *id);
+/* Waits up to timeout_s seconds (< 0 = for ever) for request id, then copies
+ * its results (arrays of info->m_count = pg_count_m(...) entries, ascending
+ * m; any may be NULL) and forgets the request.  PG_ERR_TIMEOUT if it is not
+ * done yet (it stays queued); the request's own error if it failed. */
+int pg_server_wait(pg_server *srv, uint64_t id, double timeout_s, uint64_t *ms, uint32_t *prev_gap,
+                   uint32_t *next_gap, pg_request_info *info);
+/* Id of a finished request not yet returned by this call, oldest first;
+ * PG_ERR_TIMEOUT when none finishes within timeout_s. */
+int pg_server_next_done(pg_server *srv, double timeout_s, uint64_t *id);
+int pg_server_get_stats(pg_server *srv, pg_server_stats *stats);
+/* Seconds since pg_server_create on the server clock. */
+double pg_server_clock(const pg_server *srv);
+/* Finishes the launches in flight, fails the requests not yet run
+ * (PG_ERR_STATE), stops the worker and frees the device memory. */
+int pg_server_destroy(pg_server *srv);
+
 /* Merit of a gap as overflow.cpp:162: gap / (k_log + log(m)). */
 double pg_merit(double k_log, uint64_t m, uint64_t gap);
 

@@ -16,6 +16,9 @@ Python mirror of the reference's interfaces for the hot path:
       finishing of overflow.cpp:145-188).
   merit(), format_record(), records()
       overflow.cpp:162-188.
+  Server(device).submit(p, d, sl, max_prime, m_start, m_inc) / wait(id)
+      many such searches from any thread, batched continuously on one device
+      (no counterpart in the reference, which runs one search per process).
 
 There is no CPU fallback: importing this package loads libprimegap.so and
 raises if it is missing or was built without the symbols declared in
@@ -48,6 +51,8 @@ EXPORTS = (
     "pg_job_create", "pg_job_destroy", "pg_job_get_info", "pg_job_k_words",
     "pg_count_m", "pg_sieve_interval", "pg_search", "pg_merit", "pg_format_record", "pg_next_prime_noalloc",
     "pg_search_submit", "pg_search_wait", "pg_job_stream", "pg_autotune",
+    "pg_server_create", "pg_server_submit", "pg_server_wait", "pg_server_next_done", "pg_server_get_stats",
+    "pg_server_clock", "pg_server_destroy",
 )
 PG_SEARCH_SLOTS = 2
 PG_SUBMIT_DRAIN = 0x1
@@ -92,6 +97,38 @@ class SearchStats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class ServerParams(ctypes.Structure):
+    _fields_ = [
+        ("hbm_budget", ctypes.c_uint64), ("batch_m", ctypes.c_uint32), ("window_m", ctypes.c_uint32),
+        ("max_windows", ctypes.c_uint32), ("max_sl", ctypes.c_uint32), ("small_limit", ctypes.c_uint32),
+        ("ext_window", ctypes.c_uint32), ("tpi", ctypes.c_uint32), ("pad", ctypes.c_uint32),
+    ]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [
+        ("p", ctypes.c_uint32), ("d", ctypes.c_uint32), ("sl", ctypes.c_uint32), ("rounds", ctypes.c_uint32),
+        ("max_prime", ctypes.c_uint64), ("m_start", ctypes.c_uint64), ("m_inc", ctypes.c_uint64),
+    ]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [
+        ("m_count", ctypes.c_uint64), ("k_log", ctypes.c_double), ("submit_s", ctypes.c_double),
+        ("start_s", ctypes.c_double), ("done_s", ctypes.c_double), ("windows", ctypes.c_uint32),
+        ("status", ctypes.c_int32),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("requests_done", ctypes.c_uint64), ("m_done", ctypes.c_uint64), ("prp_tests", ctypes.c_uint64),
+        ("launches", ctypes.c_uint64), ("windows", ctypes.c_uint64), ("tables_built", ctypes.c_uint64),
+        ("tables_evicted", ctypes.c_uint64), ("resident_bytes", ctypes.c_uint64), ("peak_bytes", ctypes.c_uint64),
+        ("sieve_ms", ctypes.c_double), ("prp_ms", ctypes.c_double), ("busy_s", ctypes.c_double),
+    ]
+
+
 def _load() -> ctypes.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(f"{LIB_PATH} is missing: build it with `python {PKG_DIR / 'build.py'}` "
@@ -128,6 +165,15 @@ def _load() -> ctypes.CDLL:
     lib.pg_merit.restype = ctypes.c_double
     lib.pg_merit.argtypes = [ctypes.c_double, u64, u64]
     lib.pg_format_record.argtypes = [ctypes.c_char_p, ctypes.c_size_t, u64, ctypes.c_double, u64, u32, u32, u64]
+    dbl = ctypes.c_double
+    lib.pg_server_create.argtypes = [i32, ctypes.POINTER(ServerParams), ctypes.POINTER(vp)]
+    lib.pg_server_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)]
+    lib.pg_server_wait.argtypes = [vp, u64, dbl, P64, P32, P32, ctypes.POINTER(RequestInfo)]
+    lib.pg_server_next_done.argtypes = [vp, dbl, ctypes.POINTER(ctypes.c_uint64)]
+    lib.pg_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
+    lib.pg_server_clock.restype = dbl
+    lib.pg_server_clock.argtypes = [vp]
+    lib.pg_server_destroy.argtypes = [vp]
     return lib
 
 
@@ -342,17 +388,98 @@ class Job:
 
     def records(self, res: SearchResult, min_merit: float) -> list[str]:
         """Record lines of every gap with merit > min_merit (overflow.cpp:162-188, strict >)."""
-        gaps = res.prev_gap.astype(np.float64) + res.next_gap.astype(np.float64)
-        approx = gaps / (self.k_log + np.log(res.ms.astype(np.float64)))
-        out = []
-        # numpy's log may differ from libm's in the last ulp: pre-filter with a
-        # margin, then decide with the exact formula of overflow.cpp:162
-        for i in np.nonzero(approx > min_merit - 1e-6)[0]:
-            m, pg, ng = int(res.ms[i]), int(res.prev_gap[i]), int(res.next_gap[i])
-            mer = merit(self.k_log, m, pg + ng)
-            if mer > min_merit:
-                out.append(format_record(pg + ng, mer, m, self.p, self.d, pg))
-        return out
+        return records(res, self.k_log, self.p, self.d, min_merit)
+
+
+def records(res: SearchResult, k_log: float, p: int, d: int, min_merit: float) -> list[str]:
+    """Record lines of every gap of res with merit > min_merit (overflow.cpp:162-188, strict >)."""
+    gaps = res.prev_gap.astype(np.float64) + res.next_gap.astype(np.float64)
+    approx = gaps / (k_log + np.log(np.maximum(res.ms.astype(np.float64), 1.0)))
+    out = []
+    # numpy's log may differ from libm's in the last ulp: pre-filter with a
+    # margin, then decide with the exact formula of overflow.cpp:162
+    for i in np.nonzero(approx > min_merit - 1e-6)[0]:
+        m, pg, ng = int(res.ms[i]), int(res.prev_gap[i]), int(res.next_gap[i])
+        mer = merit(k_log, m, pg + ng)
+        if mer > min_merit:
+            out.append(format_record(pg + ng, mer, m, p, d, pg))
+    return out
+
+
+@dataclasses.dataclass
+class ServedResult(SearchResult):
+    info: dict
+
+
+class Server:
+    """Continuous-batching gap search on one device (pg_server_*).
+
+    submit() queues a request of any (p, d, sl, max_prime, m range) and
+    returns its id at once; a worker thread in the library packs windows of
+    all admitted requests that share an operand layout into common search
+    launches.  wait(id) returns the request's gaps like Job.search."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0, batch_m: int = 0, window_m: int = 0,
+                 max_windows: int = 0, max_sl: int = 0, small_limit: int = 0, ext_window: int = 0, tpi: int = 0):
+        self.params = ServerParams(hbm_budget, batch_m, window_m, max_windows, max_sl, small_limit, ext_window,
+                                   tpi, 0)
+        h = ctypes.c_void_p()
+        _check(lib.pg_server_create(device, ctypes.byref(self.params), ctypes.byref(h)))
+        self._h = h
+        self._d = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.pg_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, p: int, d: int, sl: int, max_prime: int, m_start: int, m_inc: int, rounds: int = 1) -> int:
+        rq = Request(p, d, sl, rounds, max_prime, m_start, m_inc)
+        i = ctypes.c_uint64(0)
+        _check(lib.pg_server_submit(self._h, ctypes.byref(rq), ctypes.byref(i)))
+        self._d[i.value] = (d, count_m(m_start, m_inc, d))
+        return i.value
+
+    def wait(self, rid: int, timeout: float = -1.0) -> ServedResult:
+        """The request's gaps (ascending m) and its timing; raises PrimeGapError
+        with PG_ERR_TIMEOUT (-5) if it is not done within timeout seconds."""
+        _, n = self._d[rid]
+        ms = np.zeros(n, dtype=np.uint64)
+        prev = np.zeros(n, dtype=np.uint32)
+        nxt = np.zeros(n, dtype=np.uint32)
+        info = RequestInfo()
+        rc = lib.pg_server_wait(self._h, rid, timeout, _p64(ms), _p32(prev), _p32(nxt), ctypes.byref(info))
+        if rc != -5:
+            self._d.pop(rid, None)
+        _check(rc)
+        return ServedResult(ms, prev, nxt, {}, {f: getattr(info, f) for f, _ in info._fields_})
+
+    def next_done(self, timeout: float = -1.0) -> int | None:
+        """Id of the oldest finished request not yet returned here, None on timeout."""
+        i = ctypes.c_uint64(0)
+        rc = lib.pg_server_next_done(self._h, timeout, ctypes.byref(i))
+        if rc == -5:
+            return None
+        _check(rc)
+        return i.value
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib.pg_server_get_stats(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in st._fields_}
+
+    def clock(self) -> float:
+        """Seconds since the server started (the clock of the request timings)."""
+        return float(lib.pg_server_clock(self._h))
 
 
 JOB_KNOBS = ("rounds", "small_limit", "ext_window", "flags", "search_hits", "tpi")

@@ -54,7 +54,7 @@ def headers() -> list[pathlib.Path]:
 
 def units() -> list[tuple[pathlib.Path, pathlib.Path, list[str]]]:
     out = []
-    for name in ("pg_kernels", "pg_dispatch", "pg_api", "pg_noalloc"):
+    for name in ("pg_kernels", "pg_dispatch", "pg_api", "pg_server", "pg_noalloc"):
         src = CSRC / f"{name}.cu"
         if src.exists():
             out.append((src, BUILD / f"{name}.o", []))

@@ -1,13 +1,16 @@
 // pg_api.cu -- host side of the C ABI (include/primegap.h).
 //
 // Job set-up builds K = P#/d with a small host bignum (gap_common.cpp:60-65),
-// the K-prime wheel and the small-prime tables on the host, and the large
-// prime table (every prime in (small_limit, max_prime] with K mod p and
-// K^-1 mod p) on the device.  A job has PG_SEARCH_SLOTS window slots, each
-// with its own stream and buffers, so consecutive windows overlap on the
-// device.  A search of one window runs on its slot's stream:
-//   large-prime sieve -> small-prime sieve + survivor lists -> PRP search
-//   (persistent or plain) -> finalize/confirm [-> continuation launches]
+// the small-prime tables on the host, and the large prime table (every prime
+// in (small_limit, max_prime] with K mod p and K^-1 mod p) on the device.
+// These tables depend on (P, d, max_prime, small_limit) only; jobs on one
+// context with the same key share one copy whatever their sl.  A job adds
+// its K-prime wheel row and PG_SEARCH_SLOTS window slots, each with its own
+// stream and buffers, so consecutive windows overlap on the device.  A slot
+// runs one search launch over one or more windows on its stream:
+//   per window: large-prime sieve -> small-prime sieve + survivor lists
+//   then: PRP search (persistent or plain) -> finalize/confirm
+//   [-> continuation launches]
 // No function exits the process; errors come back as PG_ERR_* with a message
 // in pg_last_error().
 #include <algorithm>
@@ -19,7 +22,7 @@
 #include <string>
 #include <vector>
 
-#include "pg_internal.h"
+#include "pg_host.h"
 
 using namespace pg;
 
@@ -27,7 +30,7 @@ using namespace pg;
 
 static thread_local std::string g_last_error;
 
-static int fail(int code, const char *fmt, ...) {
+int pg::fail(int code, const char *fmt, ...) {
     char buf[512];
     va_list ap;
     va_start(ap, fmt);
@@ -37,21 +40,13 @@ static int fail(int code, const char *fmt, ...) {
     return code;
 }
 
-#define PG_CUDA(call)                                                                                    \
-    do {                                                                                                 \
-        cudaError_t e_ = (call);                                                                         \
-        if (e_ != cudaSuccess)                                                                           \
-            return fail(e_ == cudaErrorMemoryAllocation ? PG_ERR_NOMEM : PG_ERR_CUDA, "%s: %s (%s:%d)", \
-                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                              \
-    } while (0)
-
 extern "C" const char *pg_last_error(void) { return g_last_error.c_str(); }
 
 void pg::set_error(const char *msg) { g_last_error = msg; }
 
 // Timing events are recorded as external event nodes when the stream is
 // being captured, so they keep their timestamps inside a window's graph.
-static cudaError_t record_ev(cudaEvent_t e, cudaStream_t st) {
+cudaError_t pg::record_ev(cudaEvent_t e, cudaStream_t st) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaError_t err = cudaStreamIsCapturing(st, &cs);
     if (err != cudaSuccess) return err;
@@ -63,7 +58,6 @@ extern "C" const char *pg_version(void) { return "primegap-b200 0.2 (sm_100a)"; 
 
 // ======================================================= host bignum (K)
 
-typedef std::vector<uint32_t> Big;  // little-endian words, no leading zeros
 
 static void big_trim(Big &a) {
     while (!a.empty() && a.back() == 0) a.pop_back();
@@ -130,88 +124,13 @@ static bool is_prime_u32(uint32_t n) {
     return true;
 }
 
-static uint64_t gcd64(uint64_t a, uint64_t b) {
+uint64_t pg::gcd64(uint64_t a, uint64_t b) {
     while (b) {
         uint64_t t = a % b;
         a = b;
         b = t;
     }
     return a;
-}
-
-// ============================================================== objects
-
-struct pg_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    int sms = 0;
-    // PRP batch staging
-    uint32_t *d_cand = nullptr;
-    int32_t *d_res = nullptr;
-    size_t cand_cap = 0, res_cap = 0;
-};
-
-// One window in flight: its buffers, stream, events and the host state
-// needed to finish it.
-struct WinSlot {
-    cudaStream_t st = nullptr;
-    uint64_t *d_ms = nullptr;
-    int32_t *d_rank = nullptr;
-    uint32_t *d_bitmaps = nullptr;
-    uint16_t *d_lists = nullptr;
-    uint32_t *d_counts = nullptr, *d_found = nullptr, *d_kstart = nullptr, *d_knext = nullptr, *d_gaps = nullptr;
-    uint32_t *d_act0 = nullptr, *d_act1 = nullptr, *d_redo = nullptr;
-    Scalars *d_sc = nullptr;
-    Scalars *h_sc = nullptr;    // pinned
-    uint64_t *h_ms = nullptr;   // pinned
-    int32_t *h_rank = nullptr;  // pinned
-    uint32_t *h_gaps = nullptr; // pinned
-    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    cudaGraphExec_t gexec = nullptr;  // the persistent form's window graph
-    // in-flight state
-    bool busy = false;
-    uint64_t ticket = 0;
-    uint64_t m0 = 0, nodd = 0;
-    uint32_t nm = 0;
-    pg_search_stats sst{};
-};
-
-struct pg_job {
-    pg_ctx *ctx = nullptr;
-    pg_job_params prm{};
-    Big K;
-    uint32_t kbits = 0, L = 0, sly = 0, W = 0, cap = 0;
-    double k_log = 0, setup_s = 0;
-    uint32_t q1 = 0;  // small/large split: small primes are <= q1
-    // tables
-    uint32_t *d_wheel = nullptr;
-    uint32_t *d_sq = nullptr, *d_sr = nullptr;
-    uint64_t *d_sbar = nullptr;
-    uint32_t nsmall = 0;
-    uint32_t *d_tq = nullptr, *d_tr = nullptr;
-    void *d_lp = nullptr, *d_lc = nullptr, *d_lcinv = nullptr;
-    uint64_t np = 0;
-    bool wide = false;
-    // prime table index of each sieve segment (segment s starts at value seg_v0 + s * seg_span)
-    std::vector<uint64_t> seg_off;
-    uint64_t seg_v0 = 0, seg_span = 0;
-    // window slots
-    uint64_t nm_cap = 0, nodd_cap = 0;
-    WinSlot slot[PG_SEARCH_SLOTS];
-    uint64_t next_ticket = 0;
-    uint64_t dev_bytes = 0;
-    int grid = 0;
-};
-
-template <typename T>
-static int dalloc(pg_job *j, T **p, size_t count) {
-    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-    cudaError_t e = cudaMalloc((void **)p, bytes);
-    if (e != cudaSuccess)
-        return fail(e == cudaErrorMemoryAllocation ? PG_ERR_NOMEM : PG_ERR_CUDA, "cudaMalloc(%zu): %s", bytes,
-                    cudaGetErrorString(e));
-    j->dev_bytes += bytes;
-    return PG_OK;
 }
 
 // ============================================================== context
@@ -324,317 +243,313 @@ extern "C" int pg_prp_batch(pg_ctx *c, const uint32_t *limbs, uint32_t n, uint32
     return PG_OK;
 }
 
-// ================================================================= jobs
+// ================================================================ tables
 
-extern "C" uint64_t pg_count_m(uint64_t m_start, uint64_t m_inc, uint32_t d) {
-    uint64_t c = 0;
-    for (uint64_t m = m_start; m < m_start + m_inc; m++) c += gcd64(m, d) == 1;
-    return c;
-}
-
-static void slot_free(WinSlot &s) {
-    if (s.st) cudaStreamSynchronize(s.st);
-    void *ptrs[] = {s.d_ms,   s.d_rank,   s.d_bitmaps, s.d_lists, s.d_counts, s.d_found, s.d_kstart,
-                    s.d_knext, s.d_gaps,  s.d_act0,    s.d_act1,  s.d_redo,   s.d_sc};
-    for (void *p : ptrs) cudaFree(p);
-    cudaFreeHost(s.h_sc);
-    cudaFreeHost(s.h_ms);
-    cudaFreeHost(s.h_rank);
-    cudaFreeHost(s.h_gaps);
-    for (auto &e : s.ev)
-        if (e) cudaEventDestroy(e);
-    if (s.gexec) cudaGraphExecDestroy(s.gexec);
-    if (s.st) cudaStreamDestroy(s.st);
-}
-
-static void job_free(pg_job *j) {
-    if (!j) return;
-    cudaSetDevice(j->ctx->device);
-    cudaStreamSynchronize(j->ctx->stream);
-    for (auto &s : j->slot) slot_free(s);
-    void *ptrs[] = {j->d_wheel, j->d_sq, j->d_sr, j->d_sbar, j->d_tq, j->d_tr, j->d_lp, j->d_lc, j->d_lcinv};
-    for (void *p : ptrs) cudaFree(p);
-    delete j;
-}
-
-extern "C" int pg_job_destroy(pg_job *j) {
-    job_free(j);
+template <typename T>
+static int dalloc(uint64_t &acct, T **p, size_t count) {
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc((void **)p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? PG_ERR_NOMEM : PG_ERR_CUDA, "cudaMalloc(%zu): %s", bytes,
+                    cudaGetErrorString(e));
+    }
+    acct += bytes;
     return PG_OK;
+}
+
+pg::Tables::~Tables() {
+    cudaSetDevice(device);
+    void *ptrs[] = {d_sq, d_sr, d_sbar, d_tq, d_lp, d_lc, d_lcinv};
+    for (void *p : ptrs) cudaFree(p);
 }
 
 static uint32_t bitlen64(uint64_t v) { return v ? 64 - __builtin_clzll(v) : 0; }
 
-static int slot_alloc(pg_job *j, WinSlot &s) {
-    const uint64_t S = 2 * j->nm_cap;
-    int rc;
-    if ((rc = dalloc(j, &s.d_ms, j->nm_cap)) || (rc = dalloc(j, &s.d_rank, j->nodd_cap)) ||
-        (rc = dalloc(j, &s.d_bitmaps, j->nm_cap * j->W)) || (rc = dalloc(j, &s.d_lists, S * j->cap)) ||
-        (rc = dalloc(j, &s.d_counts, S)) || (rc = dalloc(j, &s.d_found, S)) || (rc = dalloc(j, &s.d_kstart, S)) ||
-        (rc = dalloc(j, &s.d_knext, S)) || (rc = dalloc(j, &s.d_gaps, S)) || (rc = dalloc(j, &s.d_act0, S)) ||
-        (rc = dalloc(j, &s.d_act1, S)) || (rc = dalloc(j, &s.d_redo, S)) || (rc = dalloc(j, &s.d_sc, 1)))
-        return rc;
-    PG_CUDA(cudaMallocHost((void **)&s.h_sc, sizeof(Scalars)));
-    PG_CUDA(cudaMallocHost((void **)&s.h_ms, j->nm_cap * 8));
-    PG_CUDA(cudaMallocHost((void **)&s.h_rank, j->nodd_cap * 4));
-    PG_CUDA(cudaMallocHost((void **)&s.h_gaps, S * 4));
-    for (auto &e : s.ev) PG_CUDA(cudaEventCreate(&e));
-    PG_CUDA(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
-    return PG_OK;
+// small primes are <= q1: max(small_limit, P), capped at the sieve limit
+static uint32_t small_bound(const pg_job_params &p) {
+    uint32_t q1 = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(p.small_limit ? p.small_limit : 65536u, p.p),
+                                               p.max_prime);
+    return std::max(q1, p.p);
 }
 
-static int job_build(pg_job *j) {
-    const pg_job_params &p = j->prm;
-    cudaStream_t st = j->ctx->stream;
+uint64_t pg::tables_bytes_estimate(const pg_job_params &p) {
+    const double x = (double)std::max<uint64_t>(p.max_prime, 17);
+    const double pi_hi = 1.26 * x / std::log(x);  // pi(x) < 1.25506 x / ln x
+    const double esz = p.max_prime >= (1ull << 32) ? 8.0 : 4.0;
+    const double q1 = small_bound(p);
+    return (uint64_t)(3.0 * esz * pi_hi + 16.0 * q1 + (1u << 20));
+}
+
+static int tables_build(pg::Tables &T, const pg_job_params &p, cudaStream_t st) {
     // ---- K = P#/d
     std::vector<uint32_t> upto_p = host_primes(p.p);
-    j->K.assign(1, 1);
-    for (uint32_t q : upto_p) big_mul_u32(j->K, q);
-    if (big_divmod_u32(j->K, p.d) != 0) return fail(PG_ERR_ARG, "d=%u does not divide %u#", p.d, p.p);
-    if (big_bits(j->K) < 2) return fail(PG_ERR_ARG, "K = %u#/%u <= 1", p.p, p.d);
-    j->kbits = big_bits(j->K);
-    if (j->K.size() > PG_MAX_WORDS - 4) return fail(PG_ERR_UNSUPPORTED, "K has %u bits", j->kbits);
-    j->k_log = big_log(j->K);
-    // every candidate must exceed max_prime (divisible then means composite)
-    if (j->kbits <= 64) {
-        uint64_t kv = 0;
-        for (size_t i = j->K.size(); i-- > 0;) kv = (kv << 32) | j->K[i];
-        if (kv <= p.max_prime + 2ull * p.sl + 2) return fail(PG_ERR_ARG, "K too small for max_prime and sl");
-    }
-    // ---- limbs of the PRP operands: N < K * (max_m + 1)
-    const uint32_t nbits = j->kbits + bitlen64(p.max_m + 1);
-    j->L = pick_layout(nbits, p.tpi);
-    if (!j->L)
-        return fail(PG_ERR_UNSUPPORTED, "operands of %u bits with tpi=%u are outside the compiled layouts", nbits,
-                    p.tpi);
-    // ---- geometry
-    j->sly = p.sl / 2;
-    j->W = (2 * j->sly + 1 + 31) / 32;
-    // ---- small primes, wheel, capacity
-    j->q1 = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(p.small_limit ? p.small_limit : 65536u, p.p), p.max_prime);
-    if (j->q1 < p.p) j->q1 = p.p;
-    const uint32_t host_lim = std::max<uint32_t>(j->q1, 1700);  // >= TRIAL_PRIMES odd primes
+    T.K.assign(1, 1);
+    for (uint32_t q : upto_p) big_mul_u32(T.K, q);
+    if (big_divmod_u32(T.K, p.d) != 0) return fail(PG_ERR_ARG, "d=%u does not divide %u#", p.d, p.p);
+    if (big_bits(T.K) < 2) return fail(PG_ERR_ARG, "K = %u#/%u <= 1", p.p, p.d);
+    T.kbits = big_bits(T.K);
+    if (T.K.size() > PG_MAX_WORDS - 4) return fail(PG_ERR_UNSUPPORTED, "K has %u bits", T.kbits);
+    T.k_log = big_log(T.K);
+    // ---- small primes, trial primes, K-primes
+    const uint32_t host_lim = std::max<uint32_t>(T.q1, 1700);  // >= TRIAL_PRIMES odd primes
     std::vector<uint32_t> sp = host_primes(host_lim);
-    std::vector<uint32_t> kprimes, sq, sr, tq, tr;
+    std::vector<uint32_t> sq, sr, tq;
     std::vector<uint64_t> sbar;
     for (uint32_t q : sp) {
         if (q == 2) continue;
-        const uint32_t c = big_mod_u32(j->K, q);
+        const uint32_t c = big_mod_u32(T.K, q);
         const uint32_t inv2 = (q + 1) / 2;
         const uint32_t r = (uint32_t)((uint64_t)((q - c) % q) * inv2 % q);  // -(K mod q)/2 mod q
         if (tq.size() < TRIAL_PRIMES) {
             tq.push_back(q);
-            tr.push_back(r);
+            T.tr.push_back(r);
         }
         if (q <= p.p && c == 0) {
-            kprimes.push_back(q);
+            T.kprimes.push_back(q);
             continue;
         }
-        if (q <= j->q1 && q <= p.max_prime) {  // odd d-primes and (P, q1]
+        if (q <= T.q1 && q <= p.max_prime) {  // odd d-primes and (P, q1]
             sq.push_back(q);
             sr.push_back(r);
             sbar.push_back(~0ull / q);
         }
     }
-    j->nsmall = (uint32_t)sq.size();
-    std::vector<uint32_t> wheel(j->W, 0);
-    auto setb = [&](uint32_t idx) { wheel[idx >> 5] |= 1u << (idx & 31); };
-    setb(j->sly);
-    for (uint32_t q : kprimes)
-        for (uint32_t idx = j->sly % q; idx <= 2 * j->sly; idx += q) setb(idx);
-    j->cap = 0;
-    for (uint32_t y = 1; y <= j->sly; y++) j->cap += !((wheel[(j->sly + y) >> 5] >> ((j->sly + y) & 31)) & 1u);
-    if (j->cap == 0) j->cap = 1;
-    // ---- device copies of the host tables
+    T.nsmall = (uint32_t)sq.size();
     int rc;
-    if ((rc = dalloc(j, &j->d_wheel, j->W)) || (rc = dalloc(j, &j->d_sq, sq.size())) ||
-        (rc = dalloc(j, &j->d_sr, sr.size())) || (rc = dalloc(j, &j->d_sbar, sbar.size())) ||
-        (rc = dalloc(j, &j->d_tq, TRIAL_PRIMES)) || (rc = dalloc(j, &j->d_tr, TRIAL_PRIMES)))
+    if ((rc = dalloc(T.bytes, &T.d_sq, sq.size())) || (rc = dalloc(T.bytes, &T.d_sr, sr.size())) ||
+        (rc = dalloc(T.bytes, &T.d_sbar, sbar.size())) || (rc = dalloc(T.bytes, &T.d_tq, TRIAL_PRIMES)))
         return rc;
-    PG_CUDA(cudaMemcpyAsync(j->d_wheel, wheel.data(), wheel.size() * 4, cudaMemcpyHostToDevice, st));
     if (!sq.empty()) {
-        PG_CUDA(cudaMemcpyAsync(j->d_sq, sq.data(), sq.size() * 4, cudaMemcpyHostToDevice, st));
-        PG_CUDA(cudaMemcpyAsync(j->d_sr, sr.data(), sr.size() * 4, cudaMemcpyHostToDevice, st));
-        PG_CUDA(cudaMemcpyAsync(j->d_sbar, sbar.data(), sbar.size() * 8, cudaMemcpyHostToDevice, st));
+        PG_CUDA(cudaMemcpyAsync(T.d_sq, sq.data(), sq.size() * 4, cudaMemcpyHostToDevice, st));
+        PG_CUDA(cudaMemcpyAsync(T.d_sr, sr.data(), sr.size() * 4, cudaMemcpyHostToDevice, st));
+        PG_CUDA(cudaMemcpyAsync(T.d_sbar, sbar.data(), sbar.size() * 8, cudaMemcpyHostToDevice, st));
     }
-    PG_CUDA(cudaMemcpyAsync(j->d_tq, tq.data(), tq.size() * 4, cudaMemcpyHostToDevice, st));
-    PG_CUDA(cudaMemcpyAsync(j->d_tr, tr.data(), tr.size() * 4, cudaMemcpyHostToDevice, st));
+    PG_CUDA(cudaMemcpyAsync(T.d_tq, tq.data(), tq.size() * 4, cudaMemcpyHostToDevice, st));
     PG_CUDA(cudaStreamSynchronize(st));  // host vectors die at return
     // ---- large primes (q1, max_prime] on the device
-    j->np = 0;
-    if (p.max_prime > j->q1) {
-        j->wide = p.max_prime >= (1ull << 32);
+    T.np = 0;
+    if (p.max_prime > T.q1) {
+        T.wide = p.max_prime >= (1ull << 32);
         const uint32_t root = (uint32_t)std::sqrt((double)p.max_prime) + 2;
         std::vector<uint32_t> base;
         for (uint32_t q : host_primes(root))
             if (q != 2) base.push_back(q);
-        const uint64_t v_first = ((uint64_t)j->q1 + 1) | 1ull;
+        const uint64_t v_first = ((uint64_t)T.q1 + 1) | 1ull;
         const uint64_t seg_span = 2ull * (1u << 18);
         const uint64_t nseg64 = (p.max_prime - v_first) / seg_span + 1;
         if (nseg64 > 0x7fffffff) return fail(PG_ERR_UNSUPPORTED, "max_prime too large");
         const uint32_t nseg = (uint32_t)nseg64;
-        uint32_t *d_base = nullptr, *d_cnt = nullptr;
+        uint32_t *d_base = nullptr, *d_cnt = nullptr, *d_K = nullptr;
         uint64_t *d_off = nullptr;
-        PG_CUDA(cudaMalloc((void **)&d_base, base.size() * 4));
-        PG_CUDA(cudaMalloc((void **)&d_cnt, (size_t)nseg * 4));
-        PG_CUDA(cudaMalloc((void **)&d_off, (size_t)nseg * 8));
-        PG_CUDA(cudaMemcpyAsync(d_base, base.data(), base.size() * 4, cudaMemcpyHostToDevice, st));
-        PG_CUDA(launch_prime_count(v_first, p.max_prime, d_base, (uint32_t)base.size(), nseg, d_cnt, st));
+        uint64_t scratch = 0;
+        auto free_scratch = [&]() {
+            cudaStreamSynchronize(st);
+            cudaFree(d_base);
+            cudaFree(d_cnt);
+            cudaFree(d_off);
+            cudaFree(d_K);
+        };
+        if ((rc = dalloc(scratch, &d_base, base.size())) || (rc = dalloc(scratch, &d_cnt, nseg)) ||
+            (rc = dalloc(scratch, &d_off, nseg)) || (rc = dalloc(scratch, &d_K, T.K.size()))) {
+            free_scratch();
+            return rc;
+        }
+        cudaError_t e = cudaMemcpyAsync(d_base, base.data(), base.size() * 4, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = launch_prime_count(v_first, p.max_prime, d_base, (uint32_t)base.size(), nseg, d_cnt, st);
         std::vector<uint32_t> cnt(nseg);
         std::vector<uint64_t> off(nseg);
-        PG_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt, (size_t)nseg * 4, cudaMemcpyDeviceToHost, st));
-        PG_CUDA(cudaStreamSynchronize(st));
+        if (e == cudaSuccess) e = cudaMemcpyAsync(cnt.data(), d_cnt, (size_t)nseg * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            free_scratch();
+            return fail(PG_ERR_CUDA, "prime count: %s", cudaGetErrorString(e));
+        }
         uint64_t acc = 0;
         for (uint32_t i = 0; i < nseg; i++) {
             off[i] = acc;
             acc += cnt[i];
         }
-        j->np = acc;
-        j->seg_off = off;
-        j->seg_v0 = v_first;
-        j->seg_span = seg_span;
-        const size_t esz = j->wide ? 8 : 4;
-        void *lp = nullptr, *lc = nullptr, *lci = nullptr;
-        cudaError_t e1 = cudaMalloc(&lp, std::max<uint64_t>(acc, 1) * esz);
-        cudaError_t e2 = cudaMalloc(&lc, std::max<uint64_t>(acc, 1) * esz);
-        cudaError_t e3 = cudaMalloc(&lci, std::max<uint64_t>(acc, 1) * esz);
-        j->d_lp = lp;
-        j->d_lc = lc;
-        j->d_lcinv = lci;
-        if (e1 || e2 || e3) {
-            cudaFree(d_base);
-            cudaFree(d_cnt);
-            cudaFree(d_off);
+        T.np = acc;
+        T.seg_off = off;
+        T.seg_v0 = v_first;
+        T.seg_span = seg_span;
+        const size_t esz = T.wide ? 8 : 4;
+        uint8_t *lp = nullptr, *lc = nullptr, *lci = nullptr;
+        if ((rc = dalloc(T.bytes, &lp, acc * esz)) || (rc = dalloc(T.bytes, &lc, acc * esz)) ||
+            (rc = dalloc(T.bytes, &lci, acc * esz))) {
+            cudaFree(lp);
+            cudaFree(lc);
+            cudaFree(lci);
+            free_scratch();
             return fail(PG_ERR_NOMEM, "prime table of %llu primes", (unsigned long long)acc);
         }
-        j->dev_bytes += 3 * std::max<uint64_t>(acc, 1) * esz;
-        PG_CUDA(cudaMemcpyAsync(d_off, off.data(), (size_t)nseg * 8, cudaMemcpyHostToDevice, st));
-        PG_CUDA(launch_prime_write(v_first, p.max_prime, d_base, (uint32_t)base.size(), nseg, d_off, j->d_lp, j->wide,
-                                   st));
-        uint32_t *d_K = nullptr;
-        PG_CUDA(cudaMalloc((void **)&d_K, j->K.size() * 4));
-        PG_CUDA(cudaMemcpyAsync(d_K, j->K.data(), j->K.size() * 4, cudaMemcpyHostToDevice, st));
-        PG_CUDA(launch_prime_tables(d_K, (uint32_t)j->K.size(), j->np, j->d_lp, j->d_lc, j->d_lcinv, j->wide, st));
-        PG_CUDA(cudaStreamSynchronize(st));
-        cudaFree(d_K);
-        cudaFree(d_base);
-        cudaFree(d_cnt);
-        cudaFree(d_off);
+        T.d_lp = lp;
+        T.d_lc = lc;
+        T.d_lcinv = lci;
+        e = cudaMemcpyAsync(d_off, off.data(), (size_t)nseg * 8, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = launch_prime_write(v_first, p.max_prime, d_base, (uint32_t)base.size(), nseg, d_off, T.d_lp, T.wide, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_K, T.K.data(), T.K.size() * 4, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = launch_prime_tables(d_K, (uint32_t)T.K.size(), T.np, T.d_lp, T.d_lc, T.d_lcinv, T.wide, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        free_scratch();
+        if (e != cudaSuccess) return fail(PG_ERR_CUDA, "prime tables: %s", cudaGetErrorString(e));
     }
-    // ---- window slots
-    const uint64_t mi = std::max<uint64_t>(p.max_m_inc, 2);
-    j->nodd_cap = mi / 2 + 1;
-    uint64_t phi = 0;
-    for (uint64_t r = 1; r <= p.d; r++) phi += gcd64(r, p.d) == 1;
-    j->nm_cap = std::min<uint64_t>(j->nodd_cap, (mi / p.d + 1) * phi);
-    if (2 * j->nm_cap >= 0xffffffffull) return fail(PG_ERR_UNSUPPORTED, "max_m_inc too large");
-    for (auto &s : j->slot)
-        if ((rc = slot_alloc(j, s))) return rc;
-    j->grid = search_grid(j->L, j->ctx->device);
     return PG_OK;
 }
 
-extern "C" int pg_job_create(pg_ctx *c, const pg_job_params *params, pg_job **out) {
-    if (!c || !params || !out) return fail(PG_ERR_ARG, "pg_job_create: NULL argument");
-    *out = nullptr;
-    const pg_job_params &p = *params;
-    if (!is_prime_u32(p.p)) return fail(PG_ERR_ARG, "p=%u is not prime", p.p);
-    if (p.d == 0 || p.d % 2) return fail(PG_ERR_ARG, "d=%u must be even", p.d);
-    if (p.sl < 2 || p.sl / 2 > 65535) return fail(PG_ERR_ARG, "sl=%u outside [2, 131071]", p.sl);
-    if (p.max_prime >= (1ull << 40)) return fail(PG_ERR_ARG, "max_prime must be < 2^40");
-    if (p.max_m == 0) return fail(PG_ERR_ARG, "max_m must be set");
-    if (p.rounds < 1 || p.rounds > 16) return fail(PG_ERR_ARG, "rounds=%u (1..16)", p.rounds);
-    PG_CUDA(cudaSetDevice(c->device));
-    const auto t0 = std::chrono::steady_clock::now();
-    pg_job *j = new pg_job();
-    j->ctx = c;
-    j->prm = p;
-    if (!j->prm.ext_window) j->prm.ext_window = 64;
-    int rc = job_build(j);
-    if (rc) {
-        std::string keep = g_last_error;
-        job_free(j);
-        g_last_error = keep;
-        return rc;
-    }
-    j->setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    *out = j;
-    return PG_OK;
-}
-
-extern "C" int pg_job_get_info(const pg_job *j, pg_job_info *info) {
-    if (!j || !info) return fail(PG_ERR_ARG, "pg_job_get_info: NULL argument");
-    info->k_bits = j->kbits;
-    info->limbs = layout_words(j->L);
-    info->tpi = j->L >> 16 ? j->L >> 16 : 1;
-    info->words_per_m = j->W;
-    info->side_capacity = j->cap;
-    info->num_primes = j->np;
-    info->num_small = j->nsmall;
-    info->k_log = j->k_log;
-    info->setup_seconds = j->setup_s;
-    info->device_bytes = j->dev_bytes;
-    return PG_OK;
-}
-
-extern "C" int pg_job_k_words(const pg_job *j, uint32_t *out, uint32_t *nwords) {
-    if (!j || !nwords) return fail(PG_ERR_ARG, "pg_job_k_words: NULL argument");
-    if (out) std::memcpy(out, j->K.data(), j->K.size() * 4);
-    *nwords = (uint32_t)j->K.size();
-    return PG_OK;
-}
-
-extern "C" void *pg_job_stream(pg_job *j, int slot) {
-    if (!j || slot < 0 || slot >= PG_SEARCH_SLOTS) return nullptr;
-    return (void *)j->slot[slot].st;
-}
-
-// ============================================================== windows
-
-// Computes the coprime m and the odd-m rank table of a window into the
-// slot's pinned staging (host work only).
-static int window_tables(pg_job *j, WinSlot &s, uint64_t m_start, uint64_t m_inc) {
-    const pg_job_params &p = j->prm;
-    if (m_inc == 0) return fail(PG_ERR_ARG, "m_inc must be > 0");
-    if (m_inc > std::max<uint64_t>(p.max_m_inc, 2))
-        return fail(PG_ERR_ARG, "m_inc=%llu > max_m_inc=%llu", (unsigned long long)m_inc,
-                    (unsigned long long)p.max_m_inc);
-    if (m_start == 0) return fail(PG_ERR_ARG, "m_start must be > 0");
-    if (m_start + m_inc - 1 > p.max_m) return fail(PG_ERR_ARG, "m beyond max_m");
-    s.m0 = m_start | 1ull;
-    const uint64_t end = m_start + m_inc;
-    s.nodd = end > s.m0 ? (end - s.m0 + 1) / 2 : 0;
-    uint32_t r = 0;
-    for (uint64_t jj = 0; jj < s.nodd; jj++) {
-        const uint64_t m = s.m0 + 2 * jj;
-        if (gcd64(m, p.d) == 1) {
-            s.h_ms[r] = m;
-            s.h_rank[jj] = (int32_t)r++;
-        } else {
-            s.h_rank[jj] = -1;
+int pg::tables_get(pg_ctx *c, const pg_job_params &p, std::shared_ptr<Tables> &out) {
+    const uint32_t q1 = small_bound(p);
+    std::lock_guard<std::mutex> lock(c->tables_mu);
+    auto &v = c->tables;
+    v.erase(std::remove_if(v.begin(), v.end(), [](const std::weak_ptr<Tables> &w) { return w.expired(); }), v.end());
+    for (auto &w : v) {
+        std::shared_ptr<Tables> t = w.lock();
+        if (t && t->p == p.p && t->d == p.d && t->max_prime == p.max_prime && t->q1 == q1) {
+            out = t;
+            return PG_OK;
         }
     }
-    s.nm = r;
+    const auto t0 = std::chrono::steady_clock::now();
+    auto t = std::make_shared<Tables>();
+    t->device = c->device;
+    t->p = p.p;
+    t->d = p.d;
+    t->max_prime = p.max_prime;
+    t->q1 = q1;
+    int rc = tables_build(*t, p, c->stream);
+    if (rc) return rc;  // t frees what it holds
+    t->setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    v.push_back(t);
+    out = t;
     return PG_OK;
 }
 
-// Uploads the window tables on the slot's stream.
-static int window_upload(WinSlot &s) {
-    if (s.nm) PG_CUDA(cudaMemcpyAsync(s.d_ms, s.h_ms, (size_t)s.nm * 8, cudaMemcpyHostToDevice, s.st));
-    if (s.nodd) PG_CUDA(cudaMemcpyAsync(s.d_rank, s.h_rank, (size_t)s.nodd * 4, cudaMemcpyHostToDevice, s.st));
+// ================================================================ slots
+
+int pg::slot_alloc(Slot &s, uint64_t nm_cap, uint64_t nodd_cap, uint64_t bm_cap, uint64_t list_cap,
+                   uint32_t win_cap) {
+    s.nm_cap = nm_cap;
+    s.nodd_cap = nodd_cap;
+    s.bm_cap = bm_cap;
+    s.list_cap = list_cap;
+    s.win_cap = win_cap;
+    const uint64_t S = 2 * nm_cap;
+    uint64_t &b = s.bytes;
+    int rc;
+    if ((rc = dalloc(b, &s.d_ms, nm_cap)) || (rc = dalloc(b, &s.d_wid, nm_cap)) ||
+        (rc = dalloc(b, &s.d_rank, nodd_cap)) || (rc = dalloc(b, &s.d_bitmaps, bm_cap)) ||
+        (rc = dalloc(b, &s.d_lists, list_cap)) || (rc = dalloc(b, &s.d_counts, S)) || (rc = dalloc(b, &s.d_found, S)) ||
+        (rc = dalloc(b, &s.d_kstart, S)) || (rc = dalloc(b, &s.d_knext, S)) || (rc = dalloc(b, &s.d_gaps, S)) ||
+        (rc = dalloc(b, &s.d_act0, S)) || (rc = dalloc(b, &s.d_act1, S)) || (rc = dalloc(b, &s.d_redo, S)) ||
+        (rc = dalloc(b, &s.d_sc, 1)) || (rc = dalloc(b, &s.d_win, win_cap)))
+        return rc;
+    PG_CUDA(cudaMallocHost((void **)&s.h_sc, sizeof(Scalars)));
+    PG_CUDA(cudaMallocHost((void **)&s.h_ms, std::max<uint64_t>(nm_cap, 1) * 8));
+    PG_CUDA(cudaMallocHost((void **)&s.h_wid, std::max<uint64_t>(nm_cap, 1) * 2));
+    PG_CUDA(cudaMallocHost((void **)&s.h_rank, std::max<uint64_t>(nodd_cap, 1) * 4));
+    PG_CUDA(cudaMallocHost((void **)&s.h_gaps, std::max<uint64_t>(S, 1) * 4));
+    PG_CUDA(cudaMallocHost((void **)&s.h_win, (size_t)std::max<uint32_t>(win_cap, 1) * sizeof(WinInfo)));
+    for (auto &e : s.ev) PG_CUDA(cudaEventCreate(&e));
+    PG_CUDA(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
     return PG_OK;
 }
 
-static int window_setup(pg_job *j, WinSlot &s, uint64_t m_start, uint64_t m_inc) {
-    int rc = window_tables(j, s, m_start, m_inc);
-    return rc ? rc : window_upload(s);
+void pg::slot_free(Slot &s) {
+    if (s.st) cudaStreamSynchronize(s.st);
+    void *ptrs[] = {s.d_ms,   s.d_wid,  s.d_rank, s.d_bitmaps, s.d_lists, s.d_counts, s.d_found, s.d_kstart,
+                    s.d_knext, s.d_gaps, s.d_act0, s.d_act1,    s.d_redo,  s.d_sc,     s.d_win};
+    for (void *p : ptrs) cudaFree(p);
+    void *hptrs[] = {s.h_sc, s.h_ms, s.h_wid, s.h_rank, s.h_gaps, s.h_win};
+    for (void *p : hptrs) cudaFreeHost(p);
+    for (auto &e : s.ev)
+        if (e) cudaEventDestroy(e);
+    if (s.gexec) cudaGraphExecDestroy(s.gexec);
+    if (s.st) cudaStreamDestroy(s.st);
+    s = Slot();
+}
+
+void pg::slot_reset(Slot &s) {
+    s.parts.clear();
+    s.nm = 0;
+    s.nodd = 0;
+    s.L = 0;
+    s.stride = 0;
+    s.ext_window = 0;
+    s.sst = pg_search_stats{};
+}
+
+bool pg::slot_fits(const Slot &s, const pg_job *j, uint64_t nm, uint64_t nodd) {
+    if (s.parts.size() >= s.win_cap) return false;
+    if (!s.parts.empty() && (j->L != s.L || j->prm.ext_window != s.ext_window)) return false;
+    if (s.nm + nm > s.nm_cap || s.nodd + nodd > s.nodd_cap) return false;
+    if (nm * j->W > s.bm_cap) return false;
+    const uint64_t stride = std::max(s.stride, j->cap);
+    return 2 * (s.nm + nm) * stride <= s.list_cap;
+}
+
+uint32_t pg::count_coprime(uint64_t m_start, uint64_t m_inc, uint32_t d, uint64_t *nodd) {
+    const uint64_t m0 = m_start | 1ull, end = m_start + m_inc;
+    const uint64_t n = end > m0 ? (end - m0 + 1) / 2 : 0;
+    uint64_t c = 0;
+    for (uint64_t i = 0; i < n; i++) c += gcd64(m0 + 2 * i, d) == 1;
+    if (nodd) *nodd = n;
+    return (uint32_t)c;
+}
+
+int pg::slot_add(Slot &s, pg_job *j, uint64_t m_start, uint64_t m_inc) {
+    const pg_job_params &p = j->prm;
+    if (m_inc == 0) return fail(PG_ERR_ARG, "m_inc must be > 0");
+    if (m_start == 0) return fail(PG_ERR_ARG, "m_start must be > 0");
+    if (m_start + m_inc - 1 > p.max_m) return fail(PG_ERR_ARG, "m beyond max_m");
+    WinPart w;
+    w.job = j;
+    w.m0 = m_start | 1ull;
+    const uint64_t end = m_start + m_inc;
+    w.nodd = end > w.m0 ? (end - w.m0 + 1) / 2 : 0;
+    w.m_off = s.nm;
+    w.odd_off = s.nodd;
+    if (s.parts.size() >= s.win_cap || s.nodd + w.nodd > s.nodd_cap) return SLOT_FULL;
+    const uint16_t wid = (uint16_t)s.parts.size();
+    // m coprime to d: odd m stepping by 2 walk the residues mod d
+    const uint8_t *cop = j->coprime.data();
+    uint32_t rm = (uint32_t)(w.m0 % p.d), r = 0;
+    int32_t *rank = s.h_rank + w.odd_off;
+    for (uint64_t jj = 0; jj < w.nodd; jj++) {
+        if (cop[rm]) {
+            if (s.nm + r >= s.nm_cap) return SLOT_FULL;
+            s.h_ms[s.nm + r] = w.m0 + 2 * jj;
+            s.h_wid[s.nm + r] = wid;
+            rank[jj] = (int32_t)r++;
+        } else {
+            rank[jj] = -1;
+        }
+        rm += 2;
+        if (rm >= p.d) rm -= p.d;
+    }
+    w.nm = r;
+    if (!slot_fits(s, j, w.nm, w.nodd)) return SLOT_FULL;
+    s.h_win[wid] = j->win;
+    if (s.parts.empty()) {
+        s.L = j->L;
+        s.ext_window = p.ext_window;
+    }
+    s.stride = std::max(s.stride, j->cap);
+    s.nm += w.nm;
+    s.nodd += w.nodd;
+    s.parts.push_back(w);
+    return PG_OK;
 }
 
 // prime-table index of the first segment starting at or above value v
-static uint64_t table_index_at(const pg_job *j, double v) {
-    if (v <= (double)j->seg_v0) return 0;
-    const double s = std::ceil((v - (double)j->seg_v0) / (double)j->seg_span);
-    if (s >= (double)j->seg_off.size()) return j->np;
-    return j->seg_off[(size_t)s];
+static uint64_t table_index_at(const pg::Tables &T, double v) {
+    if (v <= (double)T.seg_v0) return 0;
+    const double s = std::ceil((v - (double)T.seg_v0) / (double)T.seg_span);
+    if (s >= (double)T.seg_off.size()) return T.np;
+    return T.seg_off[(size_t)s];
 }
 
 // First prime-table index sieved by modular search rather than by stepping
@@ -643,87 +558,73 @@ static uint64_t table_index_at(const pg_job *j, double v) {
 // on the P=503 window); search_hits > 0 keeps primes expecting at least that
 // many hits, nodd * (2 sly + 1) / p, on the stepping kernel.
 static uint64_t large_split(const pg_job *j, uint64_t nodd) {
-    if (j->np == 0) return 0;
-    const uint64_t min_split = table_index_at(j, 2.0 * j->sly + 2);
-    if (j->prm.flags & PG_JOB_LARGE_STEP) return j->np;
+    const pg::Tables &T = *j->T;
+    if (T.np == 0) return 0;
+    const uint64_t min_split = table_index_at(T, 2.0 * j->sly + 2);
+    if (j->prm.flags & PG_JOB_LARGE_STEP) return T.np;
     if ((j->prm.flags & PG_JOB_LARGE_SEARCH) || j->prm.search_hits == 0) return min_split;
     const double hits = (double)j->prm.search_hits;
-    return std::max(min_split, table_index_at(j, (double)nodd * (2.0 * j->sly + 1) / hits));
+    return std::max(min_split, table_index_at(T, (double)nodd * (2.0 * j->sly + 1) / hits));
 }
 
-static int run_sieve(pg_job *j, WinSlot &s, bool compact) {
-    PG_CUDA(cudaMemsetAsync(s.d_bitmaps, 0, (size_t)s.nm * j->W * 4, s.st));
-    PG_CUDA(cudaMemsetAsync(&s.d_sc->max_count, 0, 4, s.st));
+// sieve of one window of the slot into its rows of lists (compact) or into
+// the bitmap rows (the slot's first window only)
+static int run_sieve(Slot &s, const WinPart &w, bool compact) {
+    const pg_job *j = w.job;
+    const pg::Tables &T = *j->T;
+    PG_CUDA(cudaMemsetAsync(s.d_bitmaps, 0, (size_t)w.nm * j->W * 4, s.st));
     LargeArgs la{};
     la.sly = j->sly;
     la.words = j->W;
-    la.m0 = s.m0;
-    la.nodd = s.nodd;
-    la.rank = s.d_rank;
+    la.m0 = w.m0;
+    la.nodd = w.nodd;
+    la.rank = s.d_rank + w.odd_off;
     la.bitmaps = s.d_bitmaps;
-    la.np = j->np;
-    la.p = j->d_lp;
-    la.cinv = j->d_lcinv;
-    la.c = j->d_lc;
-    const uint64_t split = large_split(j, s.nodd);
-    PG_CUDA(launch_sieve_large(la, j->wide, split, s.st));
-    s.sst.kernel_launches += (split > 0) + (split < j->np);
+    la.np = T.np;
+    la.p = T.d_lp;
+    la.cinv = T.d_lcinv;
+    la.c = T.d_lc;
+    const uint64_t split = large_split(j, w.nodd);
+    PG_CUDA(launch_sieve_large(la, T.wide, split, s.st));
+    s.sst.kernel_launches += (split > 0) + (split < T.np);
     SieveArgs sa{};
     sa.sly = j->sly;
     sa.words = j->W;
-    sa.cap = j->cap;
-    sa.m0 = s.m0;
-    sa.nodd = s.nodd;
-    sa.nm = s.nm;
-    sa.ms = s.d_ms;
-    sa.rank = s.d_rank;
+    sa.cap = s.stride;
+    sa.m0 = w.m0;
+    sa.nodd = w.nodd;
+    sa.nm = w.nm;
+    sa.ms = s.d_ms + w.m_off;
+    sa.rank = s.d_rank + w.odd_off;
     sa.bitmaps = s.d_bitmaps;
     sa.wheel = j->d_wheel;
-    sa.sq = j->d_sq;
-    sa.sr = j->d_sr;
-    sa.sbar = j->d_sbar;
-    sa.nsmall = j->nsmall;
-    sa.lists = s.d_lists;
-    sa.counts = s.d_counts;
+    sa.sq = T.d_sq;
+    sa.sr = T.d_sr;
+    sa.sbar = T.d_sbar;
+    sa.nsmall = T.nsmall;
+    sa.lists = s.d_lists + (size_t)2 * w.m_off * s.stride;
+    sa.counts = s.d_counts + (size_t)2 * w.m_off;
     sa.max_count = &s.d_sc->max_count;
     PG_CUDA(launch_sieve_small(sa, compact, s.st));
     s.sst.kernel_launches++;
     return PG_OK;
 }
 
-static int slot_idle(pg_job *j, WinSlot &s, const char *who) {
-    if (s.busy)
-        return fail(PG_ERR_STATE, "%s: window slot holds ticket %llu; pg_search_wait it first", who,
-                    (unsigned long long)s.ticket);
-    (void)j;
+static int slot_upload(Slot &s) {
+    if (s.nm) PG_CUDA(cudaMemcpyAsync(s.d_ms, s.h_ms, (size_t)s.nm * 8, cudaMemcpyHostToDevice, s.st));
+    if (s.nm && s.parts.size() > 1)
+        PG_CUDA(cudaMemcpyAsync(s.d_wid, s.h_wid, (size_t)s.nm * 2, cudaMemcpyHostToDevice, s.st));
+    if (s.nodd) PG_CUDA(cudaMemcpyAsync(s.d_rank, s.h_rank, (size_t)s.nodd * 4, cudaMemcpyHostToDevice, s.st));
+    PG_CUDA(cudaMemcpyAsync(s.d_win, s.h_win, s.parts.size() * sizeof(WinInfo), cudaMemcpyHostToDevice, s.st));
     return PG_OK;
 }
 
-extern "C" int pg_sieve_interval(pg_job *j, uint64_t m_start, uint64_t m_inc, uint64_t *ms, uint32_t *bitmaps) {
-    if (!j) return fail(PG_ERR_ARG, "pg_sieve_interval: job is NULL");
-    PG_CUDA(cudaSetDevice(j->ctx->device));
-    WinSlot &s = j->slot[0];
-    int rc = slot_idle(j, s, "pg_sieve_interval");
-    if (rc) return rc;
-    PG_CUDA(cudaStreamSynchronize(s.st));  // pinned staging is reused
-    if ((rc = window_setup(j, s, m_start, m_inc))) return rc;
-    if ((rc = run_sieve(j, s, false))) return rc;
-    if (bitmaps && s.nm)
-        PG_CUDA(cudaMemcpyAsync(bitmaps, s.d_bitmaps, (size_t)s.nm * j->W * 4, cudaMemcpyDeviceToHost, s.st));
-    PG_CUDA(cudaStreamSynchronize(s.st));
-    if (ms) std::memcpy(ms, s.h_ms, (size_t)s.nm * 8);
-    return PG_OK;
-}
-
-static SearchArgs base_args(pg_job *j, WinSlot &s) {
+static SearchArgs base_args(Slot &s) {
     SearchArgs a{};
-    std::memset(a.K, 0, sizeof a.K);
-    std::memcpy(a.K, j->K.data(), j->K.size() * 4);
-    a.kwords = (uint32_t)j->K.size();
-    a.sly = j->sly;
-    a.cap = j->cap;
+    a.win = s.d_win;
+    a.wid = s.parts.size() > 1 ? s.d_wid : nullptr;
+    a.cap = s.stride;
     a.ntrial = TRIAL_PRIMES;
-    a.rounds = j->prm.rounds;
     a.ms = s.d_ms;
     a.lists = s.d_lists;
     a.counts = s.d_counts;
@@ -731,16 +632,15 @@ static SearchArgs base_args(pg_job *j, WinSlot &s) {
     a.found_k = s.d_found;
     a.next_item = &s.d_sc->next_item;
     a.tests = &s.d_sc->tests;
-    a.trial_q = j->d_tq;
-    a.trial_r = j->d_tr;
+    a.trial_q = s.parts[0].job->T->d_tq;
     return a;
 }
 
 // Finalize all sides and queue the copies back; the host reads n_redo in
 // slot_finish.
-static int enqueue_finalize(pg_job *j, WinSlot &s, SearchArgs &a, uint32_t S) {
+static int enqueue_finalize(Slot &s, SearchArgs &a, uint32_t S) {
     PG_CUDA(cudaMemsetAsync(&s.d_sc->n_redo, 0, 4, s.st));
-    PG_CUDA(launch_finalize(j->L, a, S, s.d_gaps, s.d_redo, &s.d_sc->n_redo, &s.d_sc->confirm, s.d_kstart, s.st));
+    PG_CUDA(launch_finalize(s.L, a, S, s.d_gaps, s.d_redo, &s.d_sc->n_redo, &s.d_sc->confirm, s.d_kstart, s.st));
     s.sst.kernel_launches++;
     PG_CUDA(record_ev(s.ev[2], s.st));  // end of the device work (before the copies back)
     PG_CUDA(cudaMemcpyAsync(s.h_gaps, s.d_gaps, (size_t)S * 4, cudaMemcpyDeviceToHost, s.st));
@@ -748,32 +648,82 @@ static int enqueue_finalize(pg_job *j, WinSlot &s, SearchArgs &a, uint32_t S) {
     return PG_OK;
 }
 
-static int enqueue_window(pg_job *j, WinSlot &s, int form, uint32_t flags);
+// The device work of all windows on the slot's stream (capturable for the
+// persistent form; the plain form reads counts back and is not).
+static int enqueue_windows(Slot &s, int form, uint32_t flags) {
+    int rc;
+    const uint32_t S = 2 * s.nm;
+    if ((rc = slot_upload(s))) return rc;
+    PG_CUDA(record_ev(s.ev[0], s.st));
+    PG_CUDA(cudaMemsetAsync(&s.d_sc->max_count, 0, 4, s.st));
+    for (const WinPart &w : s.parts)
+        if ((rc = run_sieve(s, w, true))) return rc;
+    PG_CUDA(record_ev(s.ev[1], s.st));
+    const uint32_t warps = (uint32_t)s.grid * 4;
+    PG_CUDA(launch_init_search(S, s.d_found, s.d_kstart, s.d_act0, s.d_sc, warps, s.st));
+    s.sst.kernel_launches++;
+    SearchArgs a = base_args(s);
+    a.act = s.d_act0;
+    a.n_act = S;
+    a.ext_max = s.ext_window;
+    if (form == PG_SEARCH_PERSISTENT) {
+        a.kspan = s.stride + a.ext_max;
+        a.max_count = &s.d_sc->max_count;
+        a.unresolved = &s.d_sc->unresolved;
+        a.active_warps = &s.d_sc->active_warps;
+        if (flags & PG_SUBMIT_DRAIN) {
+            int sms = 0;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s.parts[0].job->ctx->device);
+            a.drain_lanes = 4;
+            a.min_warps = (uint32_t)sms;
+        }
+        PG_CUDA(record_ev(s.ev[3], s.st));
+        PG_CUDA(launch_search_persistent(s.L, a, s.grid, s.st));
+        PG_CUDA(record_ev(s.ev[4], s.st));
+        s.sst.kernel_launches++;
+        s.sst.passes = 1;
+    } else {  // one launch per pass, the active-side count read back after each
+        PG_CUDA(cudaMemsetAsync(s.d_knext, 0, (size_t)S * 4, s.st));
+        uint32_t n_act = S;
+        uint32_t *cur = s.d_act0, *nxt = s.d_act1;
+        PG_CUDA(record_ev(s.ev[3], s.st));
+        while (n_act > 0) {
+            a.act = cur;
+            a.n_act = n_act;
+            PG_CUDA(launch_search_plain(s.L, a, s.d_knext, s.st));
+            s.sst.passes++;
+            PG_CUDA(cudaMemsetAsync(&s.d_sc->n_out, 0, 4, s.st));
+            PG_CUDA(launch_compact_active(cur, n_act, s.d_found, s.d_knext, s.d_counts, a.ext_max, nxt,
+                                          &s.d_sc->n_out, s.st));
+            s.sst.kernel_launches += 2;
+            s.sst.d2h_bytes += 4;
+            PG_CUDA(cudaMemcpyAsync(&s.h_sc->n_out, &s.d_sc->n_out, 4, cudaMemcpyDeviceToHost, s.st));
+            PG_CUDA(cudaStreamSynchronize(s.st));
+            n_act = s.h_sc->n_out;
+            std::swap(cur, nxt);
+        }
+        PG_CUDA(record_ev(s.ev[4], s.st));
+        PG_CUDA(launch_iota(s.d_act0, S, s.st));
+        s.sst.kernel_launches++;
+    }
+    a.act = s.d_act0;
+    a.n_act = S;
+    a.max_count = nullptr;
+    return enqueue_finalize(s, a, S);
+}
 
-extern "C" int pg_search_submit(pg_job *j, uint64_t m_start, uint64_t m_inc, int form, uint32_t flags,
-                                uint64_t *ticket) {
-    if (!j || !ticket) return fail(PG_ERR_ARG, "pg_search_submit: NULL argument");
-    if (form != PG_SEARCH_PERSISTENT && form != PG_SEARCH_PLAIN)
-        return fail(PG_ERR_ARG, "pg_search_submit: form=%d", form);
-    PG_CUDA(cudaSetDevice(j->ctx->device));
-    WinSlot &s = j->slot[j->next_ticket % PG_SEARCH_SLOTS];
-    int rc = slot_idle(j, s, "pg_search_submit");
-    if (rc) return rc;
-    PG_CUDA(cudaStreamSynchronize(s.st));  // the slot's pinned staging is reused
-    s.sst = pg_search_stats{};
-    if ((rc = window_tables(j, s, m_start, m_inc))) return rc;
+int pg::slot_enqueue(Slot &s, int form, uint32_t flags, bool graph) {
     s.sst.m_count = s.nm;
-    s.sst.h2d_bytes = (uint64_t)s.nm * 8 + (uint64_t)s.nodd * 4;
-    s.ticket = j->next_ticket++;
-    s.busy = true;
-    *ticket = s.ticket;
+    s.sst.h2d_bytes = (uint64_t)s.nm * 8 + (uint64_t)s.nodd * 4 + s.parts.size() * sizeof(WinInfo) +
+                      (s.parts.size() > 1 ? (uint64_t)s.nm * 2 : 0);
     if (s.nm == 0) return PG_OK;
-    if (form == PG_SEARCH_PLAIN || (j->prm.flags & PG_JOB_NO_GRAPH)) return enqueue_window(j, s, form, flags);
+    s.grid = search_grid(s.L, s.parts[0].job->ctx->device);
+    if (form == PG_SEARCH_PLAIN || !graph) return enqueue_windows(s, form, flags);
     // The persistent form's whole window (upload, sieves, search, finalize,
     // copies back) is captured as one CUDA graph and launched once; the slot
     // keeps the instantiated graph and updates it in place for the next window.
     PG_CUDA(cudaStreamBeginCapture(s.st, cudaStreamCaptureModeThreadLocal));
-    rc = enqueue_window(j, s, form, flags);
+    int rc = enqueue_windows(s, form, flags);
     cudaGraph_t g = nullptr;
     const cudaError_t ec = cudaStreamEndCapture(s.st, &g);
     if (rc) {
@@ -798,73 +748,14 @@ extern "C" int pg_search_submit(pg_job *j, uint64_t m_start, uint64_t m_inc, int
     return PG_OK;
 }
 
-// Enqueues one window's device work on the slot's stream (capturable for the
-// persistent form; the plain form reads counts back and is not).
-static int enqueue_window(pg_job *j, WinSlot &s, int form, uint32_t flags) {
-    int rc;
-    const uint32_t S = 2 * s.nm;
-    if ((rc = window_upload(s))) return rc;
-    PG_CUDA(record_ev(s.ev[0], s.st));
-    if ((rc = run_sieve(j, s, true))) return rc;
-    PG_CUDA(record_ev(s.ev[1], s.st));
-    const uint32_t warps = (uint32_t)j->grid * 4;
-    PG_CUDA(launch_init_search(S, s.d_found, s.d_kstart, s.d_act0, s.d_sc, warps, s.st));
-    s.sst.kernel_launches++;
-    SearchArgs a = base_args(j, s);
-    a.act = s.d_act0;
-    a.n_act = S;
-    a.ext_max = j->prm.ext_window;
-    if (form == PG_SEARCH_PERSISTENT) {
-        a.kspan = j->cap + a.ext_max;
-        a.max_count = &s.d_sc->max_count;
-        a.unresolved = &s.d_sc->unresolved;
-        a.active_warps = &s.d_sc->active_warps;
-        if (flags & PG_SUBMIT_DRAIN) {
-            a.drain_lanes = 4;
-            a.min_warps = (uint32_t)j->ctx->sms;
-        }
-        PG_CUDA(record_ev(s.ev[3], s.st));
-        PG_CUDA(launch_search_persistent(j->L, a, j->grid, s.st));
-        PG_CUDA(record_ev(s.ev[4], s.st));
-        s.sst.kernel_launches++;
-        s.sst.passes = 1;
-    } else {  // one launch per pass, the active-side count read back after each
-        PG_CUDA(cudaMemsetAsync(s.d_knext, 0, (size_t)S * 4, s.st));
-        uint32_t n_act = S;
-        uint32_t *cur = s.d_act0, *nxt = s.d_act1;
-        PG_CUDA(record_ev(s.ev[3], s.st));
-        while (n_act > 0) {
-            a.act = cur;
-            a.n_act = n_act;
-            PG_CUDA(launch_search_plain(j->L, a, s.d_knext, s.st));
-            s.sst.passes++;
-            PG_CUDA(cudaMemsetAsync(&s.d_sc->n_out, 0, 4, s.st));
-            PG_CUDA(launch_compact_active(cur, n_act, s.d_found, s.d_knext, s.d_counts, a.ext_max, nxt,
-                                          &s.d_sc->n_out, s.st));
-            s.sst.kernel_launches += 2;
-            s.sst.d2h_bytes += 4;
-            PG_CUDA(cudaMemcpyAsync(&s.h_sc->n_out, &s.d_sc->n_out, 4, cudaMemcpyDeviceToHost, s.st));
-            PG_CUDA(cudaStreamSynchronize(s.st));
-            n_act = s.h_sc->n_out;
-            std::swap(cur, nxt);
-        }
-        PG_CUDA(record_ev(s.ev[4], s.st));
-        PG_CUDA(launch_iota(s.d_act0, S, s.st));
-        s.sst.kernel_launches++;
-    }
-    a.act = s.d_act0;
-    a.n_act = S;
-    a.max_count = nullptr;
-    return enqueue_finalize(j, s, a, S);
-}
-
-// Waits for the slot's queued work; continues sides without a prime within
-// sl + ext_window on the device with 4x larger extension windows.
-static int slot_finish(pg_job *j, WinSlot &s) {
+// Continues sides without a prime within sl + ext_window on the device with
+// 4x larger extension windows, then reads the timings.
+int pg::slot_finish(Slot &s) {
     PG_CUDA(cudaStreamSynchronize(s.st));
+    if (s.nm == 0) return PG_OK;
     const uint32_t S = 2 * s.nm;
-    SearchArgs a = base_args(j, s);
-    uint32_t ext_done = j->prm.ext_window;
+    SearchArgs a = base_args(s);
+    uint32_t ext_done = s.ext_window;
     for (int round = 0;; round++) {
         const uint32_t n_redo = s.h_sc->n_redo;
         if (n_redo == 0) break;
@@ -875,17 +766,17 @@ static int slot_finish(pg_job *j, WinSlot &s) {
         a.act = s.d_act1;
         a.n_act = n_redo;
         a.ext_max = ext_new;
-        a.kspan = j->cap + ext_new;
+        a.kspan = s.stride + ext_new;
         a.max_count = nullptr;
         PG_CUDA(cudaMemsetAsync(&s.d_sc->next_item, 0, 8, s.st));
-        PG_CUDA(launch_search_persistent(j->L, a, j->grid, s.st));
+        PG_CUDA(launch_search_persistent(s.L, a, s.grid, s.st));
         s.sst.kernel_launches++;
         s.sst.relaunches++;
         s.sst.extended_sides += n_redo;
         ext_done = ext_new;
         // finalize the continued sides only (their gaps and a new redo list)
         PG_CUDA(cudaMemsetAsync(&s.d_sc->n_redo, 0, 4, s.st));
-        PG_CUDA(launch_finalize(j->L, a, S, s.d_gaps, s.d_redo, &s.d_sc->n_redo, &s.d_sc->confirm, s.d_kstart, s.st));
+        PG_CUDA(launch_finalize(s.L, a, S, s.d_gaps, s.d_redo, &s.d_sc->n_redo, &s.d_sc->confirm, s.d_kstart, s.st));
         s.sst.kernel_launches++;
         PG_CUDA(record_ev(s.ev[2], s.st));
         PG_CUDA(cudaMemcpyAsync(s.h_gaps, s.d_gaps, (size_t)S * 4, cudaMemcpyDeviceToHost, s.st));
@@ -893,29 +784,7 @@ static int slot_finish(pg_job *j, WinSlot &s) {
         s.sst.d2h_bytes += 4;
         PG_CUDA(cudaStreamSynchronize(s.st));
     }
-    return PG_OK;
-}
-
-extern "C" int pg_search_wait(pg_job *j, uint64_t ticket, uint64_t *ms, uint32_t *prev_gap, uint32_t *next_gap,
-                              pg_search_stats *stats) {
-    if (!j) return fail(PG_ERR_ARG, "pg_search_wait: job is NULL");
-    PG_CUDA(cudaSetDevice(j->ctx->device));
-    WinSlot &s = j->slot[ticket % PG_SEARCH_SLOTS];
-    if (!s.busy || s.ticket != ticket)
-        return fail(PG_ERR_STATE, "pg_search_wait: ticket %llu is not in flight", (unsigned long long)ticket);
-    s.busy = false;
-    if (s.nm == 0) {
-        if (stats) *stats = s.sst;
-        return PG_OK;
-    }
-    int rc = slot_finish(j, s);
-    if (rc) return rc;
-    for (uint32_t r = 0; r < s.nm; r++) {
-        if (next_gap) next_gap[r] = s.h_gaps[2 * r];
-        if (prev_gap) prev_gap[r] = s.h_gaps[2 * r + 1];
-    }
-    if (ms) std::memcpy(ms, s.h_ms, (size_t)s.nm * 8);
-    s.sst.d2h_bytes += (uint64_t)2 * s.nm * 4 + sizeof(Scalars);
+    s.sst.d2h_bytes += (uint64_t)S * 4 + sizeof(Scalars);
     float t_sieve = 0, t_prp = 0, t_kernel = 0;
     if (cudaEventElapsedTime(&t_sieve, s.ev[0], s.ev[1]) != cudaSuccess) t_sieve = 0;
     if (cudaEventElapsedTime(&t_prp, s.ev[1], s.ev[2]) != cudaSuccess) t_prp = 0;
@@ -927,6 +796,237 @@ extern "C" int pg_search_wait(pg_job *j, uint64_t ticket, uint64_t *ms, uint32_t
     s.sst.total_ms = t_sieve + t_prp;
     s.sst.prp_tests = s.h_sc->tests;
     s.sst.confirm_tests = s.h_sc->confirm;
+    return PG_OK;
+}
+
+// ================================================================= jobs
+
+extern "C" uint64_t pg_count_m(uint64_t m_start, uint64_t m_inc, uint32_t d) {
+    uint64_t c = 0;
+    for (uint64_t m = m_start; m < m_start + m_inc; m++) c += gcd64(m, d) == 1;
+    return c;
+}
+
+static void job_free(pg_job *j) {
+    if (!j) return;
+    cudaSetDevice(j->ctx->device);
+    cudaStreamSynchronize(j->ctx->stream);
+    for (auto &s : j->slot) slot_free(s);
+    cudaFree(j->d_wheel);
+    delete j;  // drops this job's reference to the shared tables
+}
+
+extern "C" int pg_job_destroy(pg_job *j) {
+    job_free(j);
+    return PG_OK;
+}
+
+static int job_build(pg_job *j) {
+    const pg_job_params &p = j->prm;
+    int rc = tables_get(j->ctx, p, j->T);
+    if (rc) return rc;
+    const pg::Tables &T = *j->T;
+    // every candidate must exceed max_prime (divisible then means composite)
+    if (T.kbits <= 64) {
+        uint64_t kv = 0;
+        for (size_t i = T.K.size(); i-- > 0;) kv = (kv << 32) | T.K[i];
+        if (kv <= p.max_prime + 2ull * p.sl + 2) return fail(PG_ERR_ARG, "K too small for max_prime and sl");
+    }
+    // ---- limbs of the PRP operands: N < K * (max_m + 1)
+    const uint32_t nbits = T.kbits + bitlen64(p.max_m + 1);
+    j->L = pick_layout(nbits, p.tpi);
+    if (!j->L)
+        return fail(PG_ERR_UNSUPPORTED, "operands of %u bits with tpi=%u are outside the compiled layouts", nbits,
+                    p.tpi);
+    // ---- geometry, wheel, capacity
+    j->sly = p.sl / 2;
+    j->W = (2 * j->sly + 1 + 31) / 32;
+    std::vector<uint32_t> wheel(j->W, 0);
+    auto setb = [&](uint32_t idx) { wheel[idx >> 5] |= 1u << (idx & 31); };
+    setb(j->sly);
+    for (uint32_t q : T.kprimes)
+        for (uint32_t idx = j->sly % q; idx <= 2 * j->sly; idx += q) setb(idx);
+    j->cap = 0;
+    for (uint32_t y = 1; y <= j->sly; y++) j->cap += !((wheel[(j->sly + y) >> 5] >> ((j->sly + y) & 31)) & 1u);
+    if (j->cap == 0) j->cap = 1;
+    if ((rc = dalloc(j->own_bytes, &j->d_wheel, j->W))) return rc;
+    PG_CUDA(cudaMemcpyAsync(j->d_wheel, wheel.data(), wheel.size() * 4, cudaMemcpyHostToDevice, j->ctx->stream));
+    PG_CUDA(cudaStreamSynchronize(j->ctx->stream));
+    // ---- per-window constants
+    std::memset(&j->win, 0, sizeof j->win);
+    std::memcpy(j->win.K, T.K.data(), T.K.size() * 4);
+    std::memcpy(j->win.trial_r, T.tr.data(), std::min<size_t>(T.tr.size(), TRIAL_PRIMES) * 4);
+    j->win.kwords = (uint32_t)T.K.size();
+    j->win.sly = j->sly;
+    j->win.rounds = p.rounds;
+    j->coprime.assign(p.d, 0);
+    for (uint32_t r = 0; r < p.d; r++) j->coprime[r] = gcd64(r, p.d) == 1;
+    // ---- window capacity
+    const uint64_t mi = std::max<uint64_t>(p.max_m_inc, 2);
+    j->nodd_cap = mi / 2 + 1;
+    uint64_t phi = 0;
+    for (uint64_t r = 1; r <= p.d; r++) phi += gcd64(r, p.d) == 1;
+    j->nm_cap = std::min<uint64_t>(j->nodd_cap, (mi / p.d + 1) * phi);
+    if (2 * j->nm_cap >= 0xffffffffull) return fail(PG_ERR_UNSUPPORTED, "max_m_inc too large");
+    return PG_OK;
+}
+
+static int job_slots(pg_job *j) {
+    if (j->slots_ready) return PG_OK;
+    for (auto &s : j->slot) {
+        int rc = slot_alloc(s, j->nm_cap, j->nodd_cap, j->nm_cap * j->W, 2 * j->nm_cap * j->cap, 1);
+        if (rc) return rc;
+    }
+    j->slots_ready = true;
+    return PG_OK;
+}
+
+int pg::job_create(pg_ctx *c, const pg_job_params &p, pg_job **out) {
+    *out = nullptr;
+    if (!is_prime_u32(p.p)) return fail(PG_ERR_ARG, "p=%u is not prime", p.p);
+    if (p.d == 0 || p.d % 2) return fail(PG_ERR_ARG, "d=%u must be even", p.d);
+    if (p.sl < 2 || p.sl / 2 > 65535) return fail(PG_ERR_ARG, "sl=%u outside [2, 131071]", p.sl);
+    if (p.max_prime >= (1ull << 40)) return fail(PG_ERR_ARG, "max_prime must be < 2^40");
+    if (p.max_m == 0) return fail(PG_ERR_ARG, "max_m must be set");
+    if (p.rounds < 1 || p.rounds > 16) return fail(PG_ERR_ARG, "rounds=%u (1..16)", p.rounds);
+    PG_CUDA(cudaSetDevice(c->device));
+    const auto t0 = std::chrono::steady_clock::now();
+    pg_job *j = new pg_job();
+    j->ctx = c;
+    j->prm = p;
+    if (!j->prm.ext_window) j->prm.ext_window = 64;
+    int rc = job_build(j);
+    if (rc) {
+        std::string keep = g_last_error;
+        job_free(j);
+        g_last_error = keep;
+        return rc;
+    }
+    j->setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = j;
+    return PG_OK;
+}
+
+extern "C" int pg_job_create(pg_ctx *c, const pg_job_params *params, pg_job **out) {
+    if (!c || !params || !out) return fail(PG_ERR_ARG, "pg_job_create: NULL argument");
+    pg_job *j = nullptr;
+    int rc = job_create(c, *params, &j);
+    if (rc) return rc;
+    const auto t0 = std::chrono::steady_clock::now();
+    if ((rc = job_slots(j))) {
+        std::string keep = g_last_error;
+        job_free(j);
+        g_last_error = keep;
+        return rc;
+    }
+    j->setup_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = j;
+    return PG_OK;
+}
+
+extern "C" int pg_job_get_info(const pg_job *j, pg_job_info *info) {
+    if (!j || !info) return fail(PG_ERR_ARG, "pg_job_get_info: NULL argument");
+    info->k_bits = j->T->kbits;
+    info->limbs = layout_words(j->L);
+    info->tpi = j->L >> 16 ? j->L >> 16 : 1;
+    info->words_per_m = j->W;
+    info->side_capacity = j->cap;
+    info->num_primes = j->T->np;
+    info->num_small = j->T->nsmall;
+    info->k_log = j->T->k_log;
+    info->setup_seconds = j->setup_s;
+    uint64_t b = j->own_bytes + j->T->bytes;
+    for (const auto &s : j->slot) b += s.bytes;
+    info->device_bytes = b;
+    return PG_OK;
+}
+
+extern "C" int pg_job_k_words(const pg_job *j, uint32_t *out, uint32_t *nwords) {
+    if (!j || !nwords) return fail(PG_ERR_ARG, "pg_job_k_words: NULL argument");
+    if (out) std::memcpy(out, j->T->K.data(), j->T->K.size() * 4);
+    *nwords = (uint32_t)j->T->K.size();
+    return PG_OK;
+}
+
+extern "C" void *pg_job_stream(pg_job *j, int slot) {
+    if (!j || slot < 0 || slot >= PG_SEARCH_SLOTS) return nullptr;
+    return (void *)j->slot[slot].st;
+}
+
+// ============================================================== windows
+
+static int slot_idle(Slot &s, const char *who) {
+    if (s.busy)
+        return fail(PG_ERR_STATE, "%s: window slot holds ticket %llu; pg_search_wait it first", who,
+                    (unsigned long long)s.ticket);
+    return PG_OK;
+}
+
+// the job's window [m_start, m_start + m_inc) alone in slot s
+static int job_window(pg_job *j, Slot &s, uint64_t m_start, uint64_t m_inc) {
+    if (m_inc == 0) return fail(PG_ERR_ARG, "m_inc must be > 0");
+    if (m_inc > std::max<uint64_t>(j->prm.max_m_inc, 2))
+        return fail(PG_ERR_ARG, "m_inc=%llu > max_m_inc=%llu", (unsigned long long)m_inc,
+                    (unsigned long long)j->prm.max_m_inc);
+    slot_reset(s);
+    int rc = slot_add(s, j, m_start, m_inc);
+    if (rc == SLOT_FULL) return fail(PG_ERR_STATE, "window does not fit its slot");
+    return rc;
+}
+
+extern "C" int pg_sieve_interval(pg_job *j, uint64_t m_start, uint64_t m_inc, uint64_t *ms, uint32_t *bitmaps) {
+    if (!j) return fail(PG_ERR_ARG, "pg_sieve_interval: job is NULL");
+    PG_CUDA(cudaSetDevice(j->ctx->device));
+    int rc = job_slots(j);
+    if (rc) return rc;
+    Slot &s = j->slot[0];
+    if ((rc = slot_idle(s, "pg_sieve_interval"))) return rc;
+    PG_CUDA(cudaStreamSynchronize(s.st));  // pinned staging is reused
+    if ((rc = job_window(j, s, m_start, m_inc))) return rc;
+    if (s.nm == 0) return PG_OK;
+    if ((rc = slot_upload(s))) return rc;
+    if ((rc = run_sieve(s, s.parts[0], false))) return rc;
+    if (bitmaps) PG_CUDA(cudaMemcpyAsync(bitmaps, s.d_bitmaps, (size_t)s.nm * j->W * 4, cudaMemcpyDeviceToHost, s.st));
+    PG_CUDA(cudaStreamSynchronize(s.st));
+    if (ms) std::memcpy(ms, s.h_ms, (size_t)s.nm * 8);
+    return PG_OK;
+}
+
+extern "C" int pg_search_submit(pg_job *j, uint64_t m_start, uint64_t m_inc, int form, uint32_t flags,
+                                uint64_t *ticket) {
+    if (!j || !ticket) return fail(PG_ERR_ARG, "pg_search_submit: NULL argument");
+    if (form != PG_SEARCH_PERSISTENT && form != PG_SEARCH_PLAIN)
+        return fail(PG_ERR_ARG, "pg_search_submit: form=%d", form);
+    PG_CUDA(cudaSetDevice(j->ctx->device));
+    int rc = job_slots(j);
+    if (rc) return rc;
+    Slot &s = j->slot[j->next_ticket % PG_SEARCH_SLOTS];
+    if ((rc = slot_idle(s, "pg_search_submit"))) return rc;
+    PG_CUDA(cudaStreamSynchronize(s.st));  // the slot's pinned staging is reused
+    if ((rc = job_window(j, s, m_start, m_inc))) return rc;
+    s.ticket = j->next_ticket++;
+    s.busy = true;
+    *ticket = s.ticket;
+    rc = slot_enqueue(s, form, flags, !(j->prm.flags & PG_JOB_NO_GRAPH));
+    if (rc) s.busy = false;
+    return rc;
+}
+
+extern "C" int pg_search_wait(pg_job *j, uint64_t ticket, uint64_t *ms, uint32_t *prev_gap, uint32_t *next_gap,
+                              pg_search_stats *stats) {
+    if (!j) return fail(PG_ERR_ARG, "pg_search_wait: job is NULL");
+    PG_CUDA(cudaSetDevice(j->ctx->device));
+    Slot &s = j->slot[ticket % PG_SEARCH_SLOTS];
+    if (!s.busy || s.ticket != ticket)
+        return fail(PG_ERR_STATE, "pg_search_wait: ticket %llu is not in flight", (unsigned long long)ticket);
+    s.busy = false;
+    int rc = slot_finish(s);
+    if (rc) return rc;
+    for (uint32_t r = 0; r < s.nm; r++) {
+        if (next_gap) next_gap[r] = s.h_gaps[2 * r];
+        if (prev_gap) prev_gap[r] = s.h_gaps[2 * r + 1];
+    }
+    if (ms) std::memcpy(ms, s.h_ms, (size_t)s.nm * 8);
     if (stats) *stats = s.sst;
     return PG_OK;
 }

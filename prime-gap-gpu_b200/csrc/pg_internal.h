@@ -14,18 +14,29 @@ namespace pg {
 constexpr uint32_t NOT_FOUND = 0xffffffffu;
 constexpr uint32_t TRIAL_PRIMES = 256;  // odd primes tried on positions past sl
 
-// Arguments of the search kernels.  K travels in the parameter space (a
-// broadcast constant bank read) so building m*K + X costs no memory traffic.
-struct SearchArgs {
-    uint32_t K[PG_MAX_WORDS];
+// One window of a search launch: the constants of the job it belongs to.  A
+// launch may carry windows of several jobs that share an operand layout; side
+// s (m index s >> 1) belongs to window wid[s >> 1], or window 0 when wid is
+// NULL.
+struct WinInfo {
+    uint32_t K[PG_MAX_WORDS];          // K = P#/d, zero above kwords
+    uint32_t trial_r[TRIAL_PRIMES];    // (-(K mod q)/2) mod q for the trial primes
     uint32_t kwords;
-    uint32_t sly;            // sl / 2; positions Y in [-sly, sly], X = 2Y
-    uint32_t cap;            // list capacity per side
+    uint32_t sly;                      // sl / 2; positions Y in [-sly, sly], X = 2Y
+    uint32_t rounds;                   // confirmation: total bases
+    uint32_t pad;
+};
+
+// Arguments of the search kernels (one launch over the sides of one or more
+// windows; the per-side arrays are indexed by the launch's side index).
+struct SearchArgs {
+    const WinInfo *win;      // [windows]
+    const uint16_t *wid;     // [M] window of each m index, NULL = all window 0
+    uint32_t cap;            // list stride per side
     uint32_t n_act;          // active sides in this launch
     uint32_t kspan;          // items per active side in this launch
     uint32_t ext_max;        // extension positions allowed past sly (absolute)
     uint32_t ntrial;         // trial primes for extension positions
-    uint32_t rounds;         // confirmation: total bases
     const uint64_t *ms;      // m of each m index
     const uint16_t *lists;   // [2M][cap] |Y| of the survivors, nearest first
     const uint32_t *counts;  // [2M] survivors per side
@@ -36,7 +47,6 @@ struct SearchArgs {
     unsigned long long *next_item;  // work-queue head
     unsigned long long *tests;      // PRP tests executed
     const uint32_t *trial_q;   // [TRIAL_PRIMES] 3, 5, 7, ...
-    const uint32_t *trial_r;   // [TRIAL_PRIMES] (-(K mod q)/2) mod q
     // draining: a warp with no work in hand retires when more than
     // drain_lanes lanes per unresolved side are active (0 = never retire)
     uint32_t *unresolved;      // sides of this launch without a probable prime yet

@@ -38,15 +38,23 @@ __global__ void __launch_bounds__(128) k_prp_batch(const uint32_t *__restrict__ 
 
 // ------------------------------------------------------------ search core
 
-// m*K + 2Y (next side) or m*K - 2Y (prev side)
+// the window of side s
+__device__ __forceinline__ const WinInfo &win_of(const SearchArgs &a, uint32_t s) {
+    return a.win[a.wid ? a.wid[s >> 1] : 0u];
+}
+
+// m*K + 2Y (next side) or m*K - 2Y (prev side); K has at least L words
 template <int L>
-__device__ __forceinline__ void build_candidate(const SearchArgs &a, uint64_t m, uint32_t Y, bool prev,
+__device__ __forceinline__ void build_candidate(const uint32_t *__restrict__ K, uint64_t m, uint32_t Y, bool prev,
                                                 uint32_t (&x)[L]) {
+    uint32_t kw[L];
+#pragma unroll
+    for (int k = 0; k < L; k++) kw[k] = __ldg(K + k);
     const uint32_t ml = (uint32_t)m, mh = (uint32_t)(m >> 32);
     uint32_t carry = 0;
 #pragma unroll
     for (int k = 0; k < L; k++) {
-        const uint64_t p = (uint64_t)a.K[k] * ml + carry;
+        const uint64_t p = (uint64_t)kw[k] * ml + carry;
         x[k] = (uint32_t)p;
         carry = (uint32_t)(p >> 32);
     }
@@ -54,7 +62,7 @@ __device__ __forceinline__ void build_candidate(const SearchArgs &a, uint64_t m,
         carry = 0;
 #pragma unroll
         for (int k = 1; k < L; k++) {
-            const uint64_t p = (uint64_t)a.K[k - 1] * mh + x[k] + carry;
+            const uint64_t p = (uint64_t)kw[k - 1] * mh + x[k] + carry;
             x[k] = (uint32_t)p;
             carry = (uint32_t)(p >> 32);
         }
@@ -87,12 +95,13 @@ __device__ __forceinline__ bool pick_item(const SearchArgs &a, uint32_t s, uint3
     }
     const uint32_t ext = k - cnt;
     if (ext >= a.ext_max) return false;
-    Y = a.sly + 1 + ext;
+    const WinInfo &w = win_of(a, s);
+    Y = w.sly + 1 + ext;
     const uint64_t m = a.ms[s >> 1];
     const bool prev = s & 1;
     for (uint32_t i = 0; i < a.ntrial; i++) {
         const uint32_t q = a.trial_q[i];
-        const uint32_t y0 = (uint32_t)(((m % q) * a.trial_r[i]) % q);
+        const uint32_t y0 = (uint32_t)(((m % q) * w.trial_r[i]) % q);
         const uint32_t yq = Y % q;
         const uint32_t ys = prev ? (yq ? q - yq : 0u) : yq;
         if (ys == y0) return false;
@@ -102,7 +111,7 @@ __device__ __forceinline__ bool pick_item(const SearchArgs &a, uint32_t s, uint3
 
 __device__ __forceinline__ uint32_t item_y(const SearchArgs &a, uint32_t s, uint32_t k) {
     const uint32_t cnt = a.counts[s];
-    return k < cnt ? (uint32_t)a.lists[(size_t)s * a.cap + k] : a.sly + 1 + (k - cnt);
+    return k < cnt ? (uint32_t)a.lists[(size_t)s * a.cap + k] : win_of(a, s).sly + 1 + (k - cnt);
 }
 
 // Persistent search.  Items t = kk * n_act + i stand for the kk-th candidate
@@ -167,7 +176,7 @@ __global__ void __launch_bounds__(128, PG_PERSIST_MIN_BLOCKS) k_search_persisten
         if (!__any_sync(FULL, have)) break;
         if (have) {
             uint32_t x[L];
-            build_candidate<L>(a, a.ms[s >> 1], Y, s & 1, x);
+            build_candidate<L>(win_of(a, s).K, a.ms[s >> 1], Y, s & 1, x);
             const bool pr = strong_prp<L>(x, 2);
             ntests++;
             if (pr && atomicMin(&a.found_k[s], k) == NOT_FOUND && a.unresolved) atomicSub(a.unresolved, 1u);
@@ -196,7 +205,7 @@ __global__ void __launch_bounds__(128) k_search_plain(const __grid_constant__ Se
         k++;
     }
     uint32_t x[L];
-    build_candidate<L>(a, a.ms[s >> 1], Y, s & 1, x);
+    build_candidate<L>(win_of(a, s).K, a.ms[s >> 1], Y, s & 1, x);
     if (strong_prp<L>(x, 2)) a.found_k[s] = k;
     k_next[s] = k + 1;
     atomicAdd(a.tests, 1ull);
@@ -219,12 +228,13 @@ __global__ void __launch_bounds__(128) k_finalize(const __grid_constant__ Search
         return;
     }
     const uint32_t Y = item_y(a, s, k);
-    if (a.rounds > 1) {
+    const WinInfo &w = win_of(a, s);
+    if (w.rounds > 1) {
         const uint32_t bases[16] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53};
         uint32_t x[L];
-        build_candidate<L>(a, a.ms[s >> 1], Y, s & 1, x);
+        build_candidate<L>(w.K, a.ms[s >> 1], Y, s & 1, x);
         bool ok = true;
-        for (uint32_t r = 1; r < a.rounds && r < 16; r++) {
+        for (uint32_t r = 1; r < w.rounds && r < 16; r++) {
             atomicAdd(confirm_tests, 1ull);
             if (!strong_prp<L>(x, bases[r])) {
                 ok = false;

@@ -13,15 +13,15 @@ namespace pg {
 
 // the group's slice of m*K + 2Y (next side) or m*K - 2Y (prev side)
 template <int T, int LT>
-__device__ __forceinline__ void gbuild_candidate(const Group<T> &G, const SearchArgs &a, uint64_t m, uint32_t Y,
-                                                 bool prev, uint32_t (&x)[LT]) {
+__device__ __forceinline__ void gbuild_candidate(const Group<T> &G, const uint32_t *__restrict__ K, uint64_t m,
+                                                 uint32_t Y, bool prev, uint32_t (&x)[LT]) {
     const uint32_t ml = (uint32_t)m, mh = (uint32_t)(m >> 32);
     uint32_t ks[LT], kh[LT];
 #pragma unroll
     for (int k = 0; k < LT; k++) {
         const int wi = (int)(G.gl * LT) + k;
-        ks[k] = a.K[wi];
-        kh[k] = wi > 0 ? a.K[wi - 1] : 0u;  // K shifted up one word, for the high half of m
+        ks[k] = __ldg(K + wi);
+        kh[k] = wi > 0 ? __ldg(K + wi - 1) : 0u;  // K shifted up one word, for the high half of m
     }
 #pragma unroll
     for (int k = 0; k < LT; k++) x[k] = 0;
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(128) k_search_persistent_g(const __grid_consta
         if (!__any_sync(FULL, have)) break;
         if (have) {
             uint32_t x[LT];
-            gbuild_candidate<T, LT>(G, a, a.ms[s >> 1], Y, s & 1, x);
+            gbuild_candidate<T, LT>(G, win_of(a, s).K, a.ms[s >> 1], Y, s & 1, x);
             const bool pr = gstrong_prp<T, LT>(G, x, 2);
             if (G.gl == 0) {
                 ntests++;
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(128) k_search_plain_g(const __grid_constant__ 
         k++;
     }
     uint32_t x[LT];
-    gbuild_candidate<T, LT>(G, a, a.ms[s >> 1], Y, s & 1, x);
+    gbuild_candidate<T, LT>(G, win_of(a, s).K, a.ms[s >> 1], Y, s & 1, x);
     const bool pr = gstrong_prp<T, LT>(G, x, 2);
     if (G.gl == 0) {
         if (pr) a.found_k[s] = k;
@@ -195,12 +195,13 @@ __global__ void __launch_bounds__(128) k_finalize_g(const __grid_constant__ Sear
         return;
     }
     const uint32_t Y = item_y(a, s, k);
-    if (a.rounds > 1) {
+    const WinInfo &w = win_of(a, s);
+    if (w.rounds > 1) {
         const uint32_t bases[16] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53};
         uint32_t x[LT];
-        gbuild_candidate<T, LT>(G, a, a.ms[s >> 1], Y, s & 1, x);
+        gbuild_candidate<T, LT>(G, w.K, a.ms[s >> 1], Y, s & 1, x);
         bool ok = true;
-        for (uint32_t r = 1; r < a.rounds && r < 16; r++) {
+        for (uint32_t r = 1; r < w.rounds && r < 16; r++) {
             if (G.gl == 0) atomicAdd(confirm_tests, 1ull);
             if (!gstrong_prp<T, LT>(G, x, bases[r])) {
                 ok = false;

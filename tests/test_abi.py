@@ -71,3 +71,16 @@ def test_context_without_gpu_reports_an_error(pg):
         pytest.skip("a GPU is present")
     with pytest.raises(pg.PrimeGapError):
         pg.Context(0)
+
+
+def test_server_without_gpu_reports_an_error(pg):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(pg.PrimeGapError):
+        pg.Server(0)
+    import ctypes
+    rq = pg.Request(337, 2310, 1000, 1, 10**6, 10**7, 100)
+    i = ctypes.c_uint64(0)
+    assert pg.lib.pg_server_submit(None, ctypes.byref(rq), ctypes.byref(i)) == -1
+    assert pg.lib.pg_server_destroy(None) == 0
