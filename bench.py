@@ -212,7 +212,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
         stats, pending, nrec, res = [], [], 0, None
         for i in range(steps):
             pending.append(job.submit(m_start, m_inc, pg.PG_SEARCH_PERSISTENT,
-                                      pg.PG_SUBMIT_DRAIN if args.drain else 0))
+                                      (pg.PG_SUBMIT_DRAIN | (args.drain << 8)) if args.drain else 0))
             while len(pending) == pg.PG_SEARCH_SLOTS or (i == steps - 1 and pending):
                 res = job.wait(pending.pop(0))
                 stats.append(res.stats)
@@ -438,8 +438,9 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form A/B")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--drain", action="store_true",
-                    help="let the PRP kernel's warps leave as a window drains (PG_SUBMIT_DRAIN)")
+    ap.add_argument("--drain", type=int, default=32, metavar="D",
+                    help="let the PRP kernel's warps leave as a window drains, keeping D lanes per "
+                         "unresolved side (PG_SUBMIT_DRAIN; 0 = off)")
     ap.add_argument("--m-inc", type=int, default=WORKLOAD["m_inc"],
                     help="m per window (default 200000; smaller windows are for profiling only)")
     ap.add_argument("--serve", action="store_true",

@@ -216,12 +216,13 @@ int pg_next_prime_noalloc(const uint32_t *d_numbers, uint32_t n, uint32_t words,
  * t uses slot t % PG_SEARCH_SLOTS, which must not hold an un-waited ticket,
  * else PG_ERR_STATE).  pg_search_wait(ticket) blocks until that window is
  * done and fills the outputs like pg_search.  flags: PG_SUBMIT_DRAIN lets
- * the PRP kernel's warps leave once few sides remain unresolved, handing
- * their SMs to the next window (for callers that keep another window
- * submitted; a lone window finishes later with it).  pg_search() is
- * submit + wait. */
+ * the PRP kernel's warps leave once fewer than D lanes per unresolved side
+ * would remain busy, handing their SMs to the next window (for callers that
+ * keep another window submitted; a lone window finishes later with it);
+ * D = (flags >> 8) & 0xff, 0 = 4.  pg_search() is submit + wait. */
 #define PG_SEARCH_SLOTS 2
 #define PG_SUBMIT_DRAIN 0x1u
+#define PG_SUBMIT_DRAIN_LANES(d) (((uint32_t)(d) & 0xffu) << 8)
 int pg_search_submit(pg_job *job, uint64_t m_start, uint64_t m_inc, int form, uint32_t flags, uint64_t *ticket);
 int pg_search_wait(pg_job *job, uint64_t ticket, uint64_t *ms, uint32_t *prev_gap, uint32_t *next_gap,
                    pg_search_stats *stats);

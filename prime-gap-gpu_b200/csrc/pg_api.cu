@@ -659,7 +659,7 @@ static int enqueue_windows(Slot &s, int form, uint32_t flags) {
     for (const WinPart &w : s.parts)
         if ((rc = run_sieve(s, w, true))) return rc;
     PG_CUDA(record_ev(s.ev[1], s.st));
-    const uint32_t warps = (uint32_t)s.grid * 4;
+    const uint32_t warps = (uint32_t)s.grid * (PERSIST_THREADS / 32);
     PG_CUDA(launch_init_search(S, s.d_found, s.d_kstart, s.d_act0, s.d_sc, warps, s.st));
     s.sst.kernel_launches++;
     SearchArgs a = base_args(s);
@@ -674,7 +674,8 @@ static int enqueue_windows(Slot &s, int form, uint32_t flags) {
         if (flags & PG_SUBMIT_DRAIN) {
             int sms = 0;
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s.parts[0].job->ctx->device);
-            a.drain_lanes = 4;
+            const uint32_t d = (flags >> 8) & 0xffu;
+            a.drain_lanes = d ? d : 4;
             a.min_warps = (uint32_t)sms;
         }
         PG_CUDA(record_ev(s.ev[3], s.st));

@@ -13,6 +13,11 @@ namespace pg {
 
 constexpr uint32_t NOT_FOUND = 0xffffffffu;
 constexpr uint32_t TRIAL_PRIMES = 256;  // odd primes tried on positions past sl
+// The persistent search kernels run one warp per block, so a warp that
+// retires while a launch drains hands its registers back at once (a block's
+// resources are released only when all of its warps have exited) and the
+// next window's kernels can start on them.
+constexpr int PERSIST_THREADS = 32;
 
 // One window of a search launch: the constants of the job it belongs to.  A
 // launch may carry windows of several jobs that share an operand layout; side

@@ -242,104 +242,131 @@ __global__ void __launch_bounds__(256) k_sieve_large_step(const __grid_constant_
     }
 }
 
-// ------------------------------------------------- modular search, 32-bit p
+// ------------------------------------------------------ modular search
 
-// Smallest x >= 0 with (A*x + B) mod M <= W, for 0 < A < M, B < M, W < M,
-// gcd(A, M) = 1.  If B <= W, x = 0.  If W+1 >= A the first wrap (y = 1)
-// already lands in the window: x = ceil((M-B)/A).  Otherwise the first
-// wrap count y >= 1 whose interval [M*y - B, M*y - B + W] holds a multiple
-// of A solves, after the reflection z -> W - z, the same problem for
-// (M mod A, ., A, W): a Euclid step, so the depth is O(log M).  The
-// levels are kept on a small stack and x = ceil((M*y - B)/A) is rebuilt on
-// the way back.
-__device__ __forceinline__ uint32_t modsearch32(uint32_t A, uint32_t B, uint32_t M, uint32_t W) {
-    uint32_t sA[48], sB[48], sM[48];
-    int lv = 0;
-    uint64_t x;
+// For 0 < A < M, B < M, W < M - 1 and gcd(A, M) = 1, the value
+// u = (A*x + B) mod M at the smallest x >= 0 with (A*x + B) mod M <= W.
+// If B <= W, x = 0 and u = B.  If W + 1 >= A the first wrap already lands in
+// [0, W]: u = A*ceil((M-B)/A) - (M-B).  Otherwise the wrap count y whose
+// interval [M*y - B, M*y - B + W] first holds a multiple of A solves, after
+// the reflection z -> W - z, the same problem for (M mod A, ., A, W): a
+// Euclid step, so the depth is O(log M).  The landing value of each level
+// is W minus the landing value of the level below, so no state is kept on
+// the way down and nothing is rebuilt on the way back; the caller recovers
+// x = (u - B) * A^-1 mod M with one modular product.
+template <typename U>
+__device__ __forceinline__ U modsearch_value(U A, U B, U M, U W) {
+    uint32_t flips = 0;
+    U u;
     while (true) {
         if (B <= W) {
-            x = 0;
+            u = B;
             break;
         }
-        if (W + 1 >= A || lv == 48) {
-            x = (uint64_t)(M - B + A - 1) / A;
+        if (W + 1 >= A) {
+            const U t = (M - B) % A;
+            u = t ? A - t : 0;
             break;
         }
-        sA[lv] = A;
-        sB[lv] = B;
-        sM[lv] = M;
-        lv++;
-        const uint32_t r = M % A;
-        uint32_t b1 = B % A;
-        b1 = b1 >= r ? b1 - r : b1 + (A - r);      // (B - M) mod A
-        const uint32_t b2 = W >= b1 ? W - b1 : W + (A - b1);  // reflected
+        const U r = M % A;
+        U b1 = B % A;
+        b1 = b1 >= r ? b1 - r : b1 + (A - r);  // (B - M) mod A
+        B = W >= b1 ? W - b1 : W + (A - b1);   // reflected
         M = A;
         A = r;
-        B = b2;
+        flips ^= 1u;
     }
-    while (lv > 0) {
-        lv--;
-        const uint64_t y = x + 1;
-        x = ((uint64_t)sM[lv] * y - sB[lv] + sA[lv] - 1) / sA[lv];
-    }
-    return (uint32_t)x;
+    return flips ? W - u : u;
 }
 
-// Same for 64-bit moduli (primes above 2^32): products need 128 bits.
-__device__ __forceinline__ uint64_t modsearch64(uint64_t A, uint64_t B, uint64_t M, uint64_t W) {
-    uint64_t sA[64], sB[64], sM[64];
-    int lv = 0;
-    unsigned __int128 x;
+// Arithmetic mod a prime p < 2^32 with a double-precision reciprocal: the
+// quotient estimate floor(v * (1/p)) is within one of floor(v / p) for
+// every v < 2^64 and p >= 2^14 (relative error of three roundings, 3 * 2^-53,
+// times v/p <= 2^50), and the remainder is corrected in signed arithmetic.
+// Smaller p (a small-prime bound set below 2^14) take the integer remainder.
+struct Mod32 {
+    uint32_t p;
+    double inv;
+    __device__ __forceinline__ explicit Mod32(uint32_t q) : p(q), inv(1.0 / (double)q) {}
+    __device__ __forceinline__ uint32_t red(uint64_t v) const {
+        if (p < (1u << 14)) return (uint32_t)(v % p);
+        const uint64_t q = (uint64_t)((double)v * inv);
+        int64_t r = (int64_t)(v - q * p);
+        if (r < 0) r += p;
+        if (r < 0) r += p;
+        if (r >= (int64_t)p) r -= p;
+        if (r >= (int64_t)p) r -= p;
+        return (uint32_t)r;
+    }
+    __device__ __forceinline__ uint32_t mul(uint32_t a, uint32_t b) const { return red((uint64_t)a * b); }
+    __device__ __forceinline__ uint32_t sub(uint32_t a, uint32_t b) const { return a >= b ? a - b : a + (p - b); }
+};
+
+// The same for primes in [2^32, 2^40) (products of 40-bit residues split so
+// every partial product fits 64 bits).
+struct Mod40 {
+    uint64_t p;
+    __device__ __forceinline__ explicit Mod40(uint64_t q) : p(q) {}
+    __device__ __forceinline__ uint64_t red(uint64_t v) const { return v % p; }
+    __device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) const { return mulmod40(a, b, p); }
+    __device__ __forceinline__ uint64_t sub(uint64_t a, uint64_t b) const { return a >= b ? a - b : a + (p - b); }
+};
+
+// Sieve of one prime p > 2*sly + 1 over the window.  With X = 2Y and the
+// odd m = m0 + 2j, p | m*K + X  <=>  u = Y + sly = (A*j + B) mod p with
+// A = -K mod p and B = sly - m0*K/2 mod p; every j of the window with
+// u <= W = 2*sly is a hit (one per j, since p > W).  The first hit is found
+// by modsearch_value in O(log p).  When more hits are expected, the
+// three-distance structure of the sequence gives every later hit in O(1):
+// with a = the first step whose shift A*a mod p = alpha lands in [0, W] and
+// b = the first step whose shift lands in [p-W, p) (i.e. -beta), the hit
+// after u is u + alpha (step a) if that is <= W, else u - beta (step b) if
+// u >= beta, else u + alpha - beta (step a + b).  Otherwise each next hit is
+// one more search.
+template <typename U, typename Mod>
+__device__ __forceinline__ void sieve_prime(const LargeArgs &a, const Mod &md, U c, U ci) {
+    const U p = md.p;
+    const U W = (U)(2u * a.sly);
+    const U c2 = (c & 1) ? (U)((c + (uint64_t)p) >> 1) : c >> 1;  // K/2 mod p
+    const U t = md.mul(md.red(a.m0), c2);
+    U B = md.sub((U)a.sly, t);
+    const U A = p - c;     // c in [1, p)
+    const U Ainv = p - ci; // (-K)^-1
+    uint64_t j = 0;
     while (true) {
-        if (B <= W) {
-            x = 0;
-            break;
+        const U u = modsearch_value<U>(A, B, p, W);
+        j += md.mul(md.sub(u, B), Ainv);
+        if (j >= a.nodd) return;
+        mark_hit(a, j, (uint32_t)u);
+        if ((a.nodd - j - 1) * (uint64_t)(W + 1) >= 2ull * p) {  // two or more further hits expected: walk
+            const U alpha = modsearch_value<U>(A, A, p, W);
+            const uint64_t sa = 1 + (uint64_t)md.mul(md.sub(alpha, A), Ainv);
+            const U aw = A + W >= p ? A + W - p : A + W;
+            const U ub = modsearch_value<U>(A, aw, p, W - 1);
+            const U beta = W - ub;
+            const uint64_t sb = 1 + (uint64_t)md.mul(md.sub(ub, aw), Ainv);
+            U v = u;
+            while (true) {
+                if (v + alpha <= W) {
+                    j += sa;
+                    v += alpha;
+                } else if (v >= beta) {
+                    j += sb;
+                    v -= beta;
+                } else {
+                    j += sa + sb;
+                    v = v + alpha - beta;
+                }
+                if (j >= a.nodd) return;
+                mark_hit(a, j, (uint32_t)v);
+            }
         }
-        if (W + 1 >= A || lv == 64) {
-            x = (M - B + A - 1) / A;
-            break;
-        }
-        sA[lv] = A;
-        sB[lv] = B;
-        sM[lv] = M;
-        lv++;
-        const uint64_t r = M % A;
-        uint64_t b1 = B % A;
-        b1 = b1 >= r ? b1 - r : b1 + (A - r);
-        const uint64_t b2 = W >= b1 ? W - b1 : W + (A - b1);
-        M = A;
-        A = r;
-        B = b2;
+        B = u + A >= p ? u + A - p : u + A;  // residue of j + 1
+        j++;
     }
-    while (lv > 0) {
-        lv--;
-        const unsigned __int128 y = x + 1;
-        x = ((unsigned __int128)sM[lv] * y - sB[lv] + sA[lv] - 1) / sA[lv];
-    }
-    return (uint64_t)x;
 }
 
-__device__ __forceinline__ uint64_t modsearch_any(uint64_t A, uint64_t B, uint64_t p, uint64_t W) {
-    if (p < (1ull << 32)) return modsearch32((uint32_t)A, (uint32_t)B, (uint32_t)p, (uint32_t)W);
-    return modsearch64(A, B, p, W);
-}
-
-__device__ __forceinline__ uint64_t mulmod_any(uint64_t a, uint64_t b, uint64_t p) {
-    if (p < (1ull << 32)) return (a * b) % p;
-    return (uint64_t)(((unsigned __int128)a * b) % p);
-}
-
-// One thread per prime p of [first, first + count), p > 2*sly + 1.  With
-// X = 2Y and the odd m = m0 + 2j, p | m*K + X  <=>  u = Y + sly =
-// (A*j + B) mod p with A = -K mod p and B = sly - m0*K/2 mod p; every j of the
-// window with u <= W = 2*sly is a hit (one per j, since p > W).
-// The first hit is found by modsearch in O(log p).  When more hits are
-// expected, the three-distance structure of the sequence gives every later
-// hit in O(1): with a = the first step whose shift A*a mod p = alpha lands
-// in [0, W] and b = the first step whose shift lands in [p-W, p) (i.e. -beta),
-// the hit after u is u + alpha (step a) if that is <= W, else u - beta (step
-// b) if u >= beta, else u + alpha - beta (step a + b).  Otherwise each next
-// hit is one more modsearch.
+// One thread per prime of [first, first + count).
 template <typename T>
 __global__ void __launch_bounds__(256) k_sieve_large_search(const __grid_constant__ LargeArgs a, uint64_t first,
                                                             uint64_t count) {
@@ -347,45 +374,11 @@ __global__ void __launch_bounds__(256) k_sieve_large_search(const __grid_constan
     if (i >= first + count) return;
     const uint64_t p = ((const T *)a.p)[i];
     const uint64_t c = ((const T *)a.c)[i];
-    const uint64_t W = 2ull * a.sly;
-    const uint64_t inv2 = (p + 1) >> 1;
-    const uint64_t t = mulmod40(mulmod40(a.m0 % p, c, p), inv2, p);
-    const uint64_t sp = a.sly % p;
-    uint64_t B = sp >= t ? sp - t : sp + (p - t);
-    const uint64_t A = p - c;  // c in [1, p)
-    uint64_t j = 0;
-    while (j < a.nodd) {
-        const uint64_t d = modsearch_any(A, B, p, W);
-        uint64_t u = mulmod_any(A, d, p) + B;
-        if (u >= p) u -= p;
-        j += d;
-        if (j >= a.nodd) break;
-        mark_hit(a, j, (uint32_t)u);
-        if ((a.nodd - j - 1) * (W + 1) >= 2 * p) {  // two or more further hits expected: walk
-            const uint64_t sa = 1 + modsearch_any(A, A, p, W);
-            const uint64_t alpha = mulmod_any(A, sa, p);
-            const uint64_t aw = A + W >= p ? A + W - p : A + W;
-            const uint64_t sb = 1 + modsearch_any(A, aw, p, W - 1);
-            const uint64_t beta = p - mulmod_any(A, sb, p);
-            while (true) {
-                if (u + alpha <= W) {
-                    j += sa;
-                    u += alpha;
-                } else if (u >= beta) {
-                    j += sb;
-                    u -= beta;
-                } else {
-                    j += sa + sb;
-                    u = u + alpha - beta;
-                }
-                if (j >= a.nodd) break;
-                mark_hit(a, j, (uint32_t)u);
-            }
-            break;
-        }
-        B = u + A >= p ? u + A - p : u + A;  // residue of j + 1
-        j++;
-    }
+    const uint64_t ci = ((const T *)a.cinv)[i];
+    if (p < (1ull << 32))
+        sieve_prime<uint32_t, Mod32>(a, Mod32((uint32_t)p), (uint32_t)c, (uint32_t)ci);
+    else
+        sieve_prime<uint64_t, Mod40>(a, Mod40(p), c, ci);
 }
 
 cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, cudaStream_t st) {

@@ -15,7 +15,7 @@
 #include "pg_internal.h"
 #include "pg_mont.cuh"
 
-// minimum resident 128-thread blocks per SM requested from ptxas for the
+// minimum resident one-warp blocks per SM requested from ptxas for the
 // persistent search (caps its registers); 1 leaves the choice to ptxas
 #ifndef PG_PERSIST_MIN_BLOCKS
 #define PG_PERSIST_MIN_BLOCKS 1
@@ -123,7 +123,7 @@ __device__ __forceinline__ uint32_t item_y(const SearchArgs &a, uint32_t s, uint
 // A side is resolved by the smallest k with a probable prime: every smaller
 // k is tested because items are only skipped behind a smaller found k.
 template <int L>
-__global__ void __launch_bounds__(128, PG_PERSIST_MIN_BLOCKS) k_search_persistent(const __grid_constant__ SearchArgs a) {
+__global__ void __launch_bounds__(PERSIST_THREADS, PG_PERSIST_MIN_BLOCKS) k_search_persistent(const __grid_constant__ SearchArgs a) {
     const unsigned FULL = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31;
     uint32_t kspan = a.kspan;
@@ -266,13 +266,13 @@ cudaError_t launch_prp_batch_t(const uint32_t *cand, uint32_t words, uint32_t n,
 template <int L>
 int search_occupancy_t() {
     int per = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_search_persistent<L>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_search_persistent<L>, PERSIST_THREADS, 0);
     return per;
 }
 
 template <int L>
 cudaError_t launch_search_persistent_t(const SearchArgs &a, int grid, cudaStream_t st) {
-    k_search_persistent<L><<<grid, 128, 0, st>>>(a);
+    k_search_persistent<L><<<grid, PERSIST_THREADS, 0, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(128) k_prp_batch_g(const uint32_t *__restrict_
 
 // Persistent search with one item per group (see k_search_persistent).
 template <int T, int LT>
-__global__ void __launch_bounds__(128) k_search_persistent_g(const __grid_constant__ SearchArgs a) {
+__global__ void __launch_bounds__(PERSIST_THREADS) k_search_persistent_g(const __grid_constant__ SearchArgs a) {
     const unsigned FULL = 0xffffffffu;
     const Group<T> G;
     uint32_t kspan = a.kspan;
@@ -234,13 +234,13 @@ cudaError_t glaunch_prp_batch(const uint32_t *cand, uint32_t words, uint32_t n, 
 template <int T, int LT>
 int gsearch_occupancy() {
     int per = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_search_persistent_g<T, LT>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_search_persistent_g<T, LT>, PERSIST_THREADS, 0);
     return per;
 }
 
 template <int T, int LT>
 cudaError_t glaunch_search_persistent(const SearchArgs &a, int grid, cudaStream_t st) {
-    k_search_persistent_g<T, LT><<<grid, 128, 0, st>>>(a);
+    k_search_persistent_g<T, LT><<<grid, PERSIST_THREADS, 0, st>>>(a);
     return cudaGetLastError();
 }
 
