@@ -292,7 +292,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
         "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": workload_name(RANK_STARTS[0], m_inc),
-                   "form": f"persistent, {pg.PG_SEARCH_SLOTS} windows in flight",
+                   "form": f"persistent, {pg.PG_SEARCH_SLOTS} windows in flight"
+                           + (f", draining to {args.drain} lanes per unresolved side" if args.drain else ""),
                    "m_per_gpu_per_step": m_count, "sl": W["sl"], "max_prime": W["max_prime"],
                    "limbs": job.info["limbs"], "parallelism": f"weak: {world} disjoint m-windows",
                    "l2": "inputs larger than L2 (786 MB prime tables read every step)"},
