@@ -212,7 +212,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
         stats, pending, nrec, res = [], [], 0, None
         for i in range(steps):
             pending.append(job.submit(m_start, m_inc, pg.PG_SEARCH_PERSISTENT,
-                                      (pg.PG_SUBMIT_DRAIN | (args.drain << 8)) if args.drain else 0))
+                                      ((pg.PG_SUBMIT_DRAIN | (args.drain << 8)) if args.drain else 0)
+                                      | (args.warps_per_sm << 16)))
             while len(pending) == pg.PG_SEARCH_SLOTS or (i == steps - 1 and pending):
                 res = job.wait(pending.pop(0))
                 stats.append(res.stats)
@@ -293,6 +294,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": workload_name(RANK_STARTS[0], m_inc),
                    "form": f"persistent, {pg.PG_SEARCH_SLOTS} windows in flight"
+                           + (f", {args.warps_per_sm} PRP warps per SM per window" if args.warps_per_sm else "")
                            + (f", draining to {args.drain} lanes per unresolved side" if args.drain else ""),
                    "m_per_gpu_per_step": m_count, "sl": W["sl"], "max_prime": W["max_prime"],
                    "limbs": job.info["limbs"], "parallelism": f"weak: {world} disjoint m-windows",
@@ -379,7 +381,7 @@ def run_serve(args) -> dict:
     reqs = serve_requests(args.serve_jobs)
     classes = sorted({(p, d) for p, d, *_ in reqs})
     max_sl = max(r[2] for r in reqs)
-    with pg.Server(0, max_sl=max_sl) as srv:
+    with pg.Server(0, max_sl=max_sl, warps_per_sm=args.warps_per_sm) as srv:
         # resident tables for every (P, d) first: one small request per class
         warm = [srv.submit(p, d, 1_000, reqs[0][3], 1_000_001, 200) for p, d in classes]
         t = time.perf_counter()
@@ -427,7 +429,7 @@ def run_serve(args) -> dict:
         "n_gpus": 1, "data": "synthetic (seeded request mix)",
         "config": {"workload": f"{len(reqs)} requests, P in {{337,503,907}}, d in {{210,2190,2310}}, "
                                "500-20000 m from [1e6,1e9], SL=round(8 ln N), primes <= 1e9",
-                   "seed": SERVE_SEED},
+                   "seed": SERVE_SEED, "warps_per_sm": args.warps_per_sm},
     }
 
 
@@ -439,15 +441,22 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form A/B")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--drain", type=int, default=32, metavar="D",
+    ap.add_argument("--drain", type=int, default=0, metavar="D",
                     help="let the PRP kernel's warps leave as a window drains, keeping D lanes per "
                          "unresolved side (PG_SUBMIT_DRAIN; 0 = off)")
+    ap.add_argument("--warps-per-sm", type=int, default=None, metavar="W",
+                    help="cap each launch's PRP kernel at W resident warps per SM so the two launches "
+                         "in flight run side by side (0 = as many as fit; default 6 for the window "
+                         "benchmark, measured best at 22 words, and 0 for --serve, whose launches are "
+                         "large enough that the cap costs more than it saves)")
     ap.add_argument("--m-inc", type=int, default=WORKLOAD["m_inc"],
                     help="m per window (default 200000; smaller windows are for profiling only)")
     ap.add_argument("--serve", action="store_true",
                     help="the serving workload instead: p50/p99 latency of a request mix (pg_server_*)")
     ap.add_argument("--serve-jobs", type=int, default=256)
     args = ap.parse_args(argv)
+    if args.warps_per_sm is None:
+        args.warps_per_sm = 0 if args.serve else 6
     if args.serve:
         print(json.dumps(run_serve(args)), flush=True)
         return 0

@@ -129,8 +129,10 @@ typedef struct {
     uint64_t num_primes;      /* primes in (P, max_prime] */
     uint64_t num_small;       /* of them (plus odd d-primes) sieved per m */
     double k_log;             /* log(K), as _log (gap_common.cpp:44-48) */
-    double setup_seconds;     /* wall time of pg_job_create */
-    uint64_t device_bytes;    /* device memory held by the job */
+    double setup_seconds;     /* wall time of pg_job_create (small when the tables were shared) */
+    uint64_t device_bytes;    /* device memory the job uses: its slots and wheel, and the prime
+                                 tables it shares with the context's jobs of the same
+                                 (p, d, max_prime, small_limit) */
 } pg_job_info;
 
 int pg_job_create(pg_ctx *ctx, const pg_job_params *params, pg_job **out);
@@ -219,10 +221,13 @@ int pg_next_prime_noalloc(const uint32_t *d_numbers, uint32_t n, uint32_t words,
  * the PRP kernel's warps leave once fewer than D lanes per unresolved side
  * would remain busy, handing their SMs to the next window (for callers that
  * keep another window submitted; a lone window finishes later with it);
- * D = (flags >> 8) & 0xff, 0 = 4.  pg_search() is submit + wait. */
+ * D = (flags >> 8) & 0xff, 0 = 4.  PG_SUBMIT_WARPS_PER_SM(w) caps the PRP
+ * kernel at w resident warps per SM (0 = as many as fit), leaving room for
+ * the next window's kernels to run beside it.  pg_search() is submit + wait. */
 #define PG_SEARCH_SLOTS 2
 #define PG_SUBMIT_DRAIN 0x1u
 #define PG_SUBMIT_DRAIN_LANES(d) (((uint32_t)(d) & 0xffu) << 8)
+#define PG_SUBMIT_WARPS_PER_SM(w) (((uint32_t)(w) & 0xffu) << 16)
 int pg_search_submit(pg_job *job, uint64_t m_start, uint64_t m_inc, int form, uint32_t flags, uint64_t *ticket);
 int pg_search_wait(pg_job *job, uint64_t ticket, uint64_t *ms, uint32_t *prev_gap, uint32_t *next_gap,
                    pg_search_stats *stats);
@@ -263,7 +268,8 @@ typedef struct {
     uint32_t small_limit;  /* as pg_job_params (0 = default) */
     uint32_t ext_window;   /* as pg_job_params (0 = default) */
     uint32_t tpi;          /* as pg_job_params (0 = automatic) */
-    uint32_t pad;
+    uint32_t warps_per_sm; /* cap on each launch's PRP warps per SM (PG_SUBMIT_WARPS_PER_SM), so the
+                              two launches in flight share the SMs; 0 = as many as fit */
 } pg_server_params;
 
 typedef struct {

@@ -58,6 +58,14 @@ PG_SEARCH_SLOTS = 2
 PG_SUBMIT_DRAIN = 0x1
 
 
+def PG_SUBMIT_DRAIN_LANES(d: int) -> int:
+    return (d & 0xff) << 8
+
+
+def PG_SUBMIT_WARPS_PER_SM(w: int) -> int:
+    return (w & 0xff) << 16
+
+
 class PrimeGapError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"libprimegap error {code}: {msg}")
@@ -101,7 +109,7 @@ class ServerParams(ctypes.Structure):
     _fields_ = [
         ("hbm_budget", ctypes.c_uint64), ("batch_m", ctypes.c_uint32), ("window_m", ctypes.c_uint32),
         ("max_windows", ctypes.c_uint32), ("max_sl", ctypes.c_uint32), ("small_limit", ctypes.c_uint32),
-        ("ext_window", ctypes.c_uint32), ("tpi", ctypes.c_uint32), ("pad", ctypes.c_uint32),
+        ("ext_window", ctypes.c_uint32), ("tpi", ctypes.c_uint32), ("warps_per_sm", ctypes.c_uint32),
     ]
 
 
@@ -420,9 +428,10 @@ class Server:
     launches.  wait(id) returns the request's gaps like Job.search."""
 
     def __init__(self, device: int = 0, hbm_budget: int = 0, batch_m: int = 0, window_m: int = 0,
-                 max_windows: int = 0, max_sl: int = 0, small_limit: int = 0, ext_window: int = 0, tpi: int = 0):
+                 max_windows: int = 0, max_sl: int = 0, small_limit: int = 0, ext_window: int = 0, tpi: int = 0,
+                 warps_per_sm: int = 0):
         self.params = ServerParams(hbm_budget, batch_m, window_m, max_windows, max_sl, small_limit, ext_window,
-                                   tpi, 0)
+                                   tpi, warps_per_sm)
         h = ctypes.c_void_p()
         _check(lib.pg_server_create(device, ctypes.byref(self.params), ctypes.byref(h)))
         self._h = h

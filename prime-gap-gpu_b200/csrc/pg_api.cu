@@ -719,6 +719,8 @@ int pg::slot_enqueue(Slot &s, int form, uint32_t flags, bool graph) {
                       (s.parts.size() > 1 ? (uint64_t)s.nm * 2 : 0);
     if (s.nm == 0) return PG_OK;
     s.grid = search_grid(s.L, s.parts[0].job->ctx->device);
+    const uint32_t wps = (flags >> 16) & 0xffu;  // warps per SM cap
+    if (wps) s.grid = std::min(s.grid, s.parts[0].job->ctx->sms * (int)wps * 32 / PERSIST_THREADS);
     if (form == PG_SEARCH_PLAIN || !graph) return enqueue_windows(s, form, flags);
     // The persistent form's whole window (upload, sieves, search, finalize,
     // copies back) is captured as one CUDA graph and launched once; the slot

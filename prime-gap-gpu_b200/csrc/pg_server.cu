@@ -382,7 +382,7 @@ struct pg_server {
                 if (ss.inflight || stop) continue;
                 if (!fill(ss)) break;
                 ss.seq = ++launch_seq;
-                int rc = slot_enqueue(ss.s, PG_SEARCH_PERSISTENT, 0, false);
+                int rc = slot_enqueue(ss.s, PG_SEARCH_PERSISTENT, PG_SUBMIT_WARPS_PER_SM(prm.warps_per_sm), false);
                 if (rc) {
                     fail_launch(ss, rc, pg_last_error());
                     continue;
