@@ -84,133 +84,165 @@ __device__ __forceinline__ uint32_t neg_inv32(uint32_t n0) {
 }
 
 // ------------------------------------------------------------ Montgomery
+//
+// Register layout.  The fused 32x32+64 multiply-add writes a 64-bit pair of
+// registers that must be aligned, so a single accumulator array whose chains
+// start at both even and odd word positions costs register moves on every
+// product of the odd-aligned chains.  Instead the running value is kept as
+//     E + F*B + C*B^L          (B = 2^32)
+// with products whose low word lands at an even position accumulated in E
+// (pairs E[p], E[p+1]) and those landing at an odd position in F (F[k] holds
+// position k+1, pairs F[p-1], F[p]): every multiply-add of every chain works
+// on an aligned pair.  C counts the carries out of the reduction's chains
+// (positions L .. 2L) so they never ripple.  The sums that resolve a word
+// from E, F and the carry below are written as PTX carry chains too: left to
+// the compiler they interleave with the multiply chains and force the carry
+// flag through general registers.
+
+// (lo, hi) += a*b as one link of a carry chain (FIRST: no carry in)
+template <bool FIRST>
+__device__ __forceinline__ void mad_link(uint32_t &lo, uint32_t &hi, uint32_t a, uint32_t b) {
+    lo = FIRST ? mad_lo_cc(a, b, lo) : madc_lo_cc(a, b, lo);
+    hi = madc_hi_cc(a, b, hi);
+}
+
+// x = (E + F*B) * R^-1 mod n for E + F*B < n*R (x < n), R = B^L.
+template <int L>
+__device__ __forceinline__ void mont_redc_ef(uint32_t (&E)[2 * L + 2], uint32_t (&F)[2 * L + 2],
+                                             const uint32_t (&n)[L], uint32_t ninv, uint32_t (&x)[L]) {
+    uint32_t C[L + 2];
+#pragma unroll
+    for (int k = 0; k < L + 2; k++) C[k] = 0;
+    uint32_t cin = 0;  // carry into position i from the resolved positions below
+#pragma unroll
+    for (int i = 0; i < L; i++) {
+        uint32_t w = E[i];  // word i of the running value
+        if (i) {
+            w = add_cc(E[i], F[i - 1]);
+            w = add_cc(w, cin);
+        }
+        const uint32_t q = w * ninv;
+        // chain over E (j with i + j even) and chain over F (i + j odd); each
+        // chain's carry out is counted in C at its position (>= L)
+#pragma unroll
+        for (int par = 0; par < 2; par++) {
+            const int j0 = (i + par) & 1;
+            int jl = j0;
+#pragma unroll
+            for (int j = j0; j < L; j += 2) jl = j;
+#pragma unroll
+            for (int j = j0; j < L; j += 2) {
+                const int p = i + j;
+                if (par == 0) {
+                    if (j == j0) mad_link<true>(E[p], E[p + 1], q, n[j]);
+                    else mad_link<false>(E[p], E[p + 1], q, n[j]);
+                } else {
+                    if (j == j0) mad_link<true>(F[p - 1], F[p], q, n[j]);
+                    else mad_link<false>(F[p - 1], F[p], q, n[j]);
+                }
+            }
+            const int cp = i + jl + 2;
+            if (cp <= 2 * L) C[cp - L] = addc(C[cp - L], 0u);
+        }
+        // position i now sums to a multiple of B (the REDC identity); its carry
+        // (0..2) moves up.  At i = 0 the carry went up inside the pair add.
+        if (i) {
+            const uint32_t z = add_cc(E[i], F[i - 1]);
+            const uint32_t k1 = addc(0u, 0u);
+            (void)add_cc(z, cin);
+            cin = addc(k1, 0u);
+        }
+    }
+    // u = positions L .. 2L of the sum (u < 2n), then x = u mod n
+    C[0] += cin;
+    uint32_t A[L + 1], u[L + 1];
+    A[0] = add_cc(E[L], F[L - 1]);
+#pragma unroll
+    for (int k = 1; k < L; k++) A[k] = addc_cc(E[L + k], F[L + k - 1]);
+    A[L] = addc(E[2 * L], F[2 * L - 1]);
+    u[0] = add_cc(A[0], C[0]);
+#pragma unroll
+    for (int k = 1; k < L; k++) u[k] = addc_cc(A[k], C[k]);
+    u[L] = addc(A[L], C[L]);
+    uint32_t d[L];
+    d[0] = sub_cc(u[0], n[0]);
+#pragma unroll
+    for (int k = 1; k < L; k++) d[k] = subc_cc(u[k], n[k]);
+    const uint32_t top = subc(u[L], 0u);  // 0 if u >= n, 0xffffffff on borrow
+    const bool keep = top != 0;
+#pragma unroll
+    for (int k = 0; k < L; k++) x[k] = keep ? u[k] : d[k];
+}
+
 // REDC of the 2L+1 word value t (< n*R): returns t * R^-1 mod n in x (< n).
 template <int L>
 __device__ __forceinline__ void mont_redc(uint32_t (&t)[2 * L + 1], const uint32_t (&n)[L], uint32_t ninv,
                                           uint32_t (&x)[L]) {
-    uint32_t pend = 0;  // carry pending into t[i + L]
+    uint32_t E[2 * L + 2], F[2 * L + 2];
 #pragma unroll
-    for (int i = 0; i < L; i++) {
-        const uint32_t q = t[i] * ninv;
-        // The chain that ends at word i+L-1 ("short") runs first, then the
-        // pending carry and its carry go into t[i+L], then the chain that
-        // ends at word i+L ("long").  Even j: lo at i+j, hi at i+j+1.
-        if ((L & 1) == 0) {
-            // short = even j (last even j = L-2 -> hi at i+L-1)
-            t[i] = mad_lo_cc(q, n[0], t[i]);
-            t[i + 1] = madc_hi_cc(q, n[0], t[i + 1]);
-#pragma unroll
-            for (int j = 2; j < L; j += 2) {
-                t[i + j] = madc_lo_cc(q, n[j], t[i + j]);
-                t[i + j + 1] = madc_hi_cc(q, n[j], t[i + j + 1]);
-            }
-            t[i + L] = addc_cc(t[i + L], pend);
-            uint32_t c1 = addc(0u, 0u);
-            // long = odd j (last odd j = L-1 -> hi at i+L)
-            t[i + 1] = mad_lo_cc(q, n[1], t[i + 1]);
-            t[i + 2] = madc_hi_cc(q, n[1], t[i + 2]);
-#pragma unroll
-            for (int j = 3; j < L; j += 2) {
-                t[i + j] = madc_lo_cc(q, n[j], t[i + j]);
-                t[i + j + 1] = madc_hi_cc(q, n[j], t[i + j + 1]);
-            }
-            pend = addc(c1, 0u);
-        } else {
-            // short = odd j (last odd j = L-2 -> hi at i+L-1)
-            if (L > 1) {
-                t[i + 1] = mad_lo_cc(q, n[1 < L ? 1 : 0], t[i + 1]);
-                t[i + 2] = madc_hi_cc(q, n[1 < L ? 1 : 0], t[i + 2]);
-#pragma unroll
-                for (int j = 3; j < L; j += 2) {
-                    t[i + j] = madc_lo_cc(q, n[j], t[i + j]);
-                    t[i + j + 1] = madc_hi_cc(q, n[j], t[i + j + 1]);
-                }
-                t[i + L] = addc_cc(t[i + L], pend);
-            } else {
-                t[i + L] = add_cc(t[i + L], pend);
-            }
-            uint32_t c1 = addc(0u, 0u);
-            // long = even j (last even j = L-1 -> hi at i+L)
-            t[i] = mad_lo_cc(q, n[0], t[i]);
-            t[i + 1] = madc_hi_cc(q, n[0], t[i + 1]);
-#pragma unroll
-            for (int j = 2; j < L; j += 2) {
-                t[i + j] = madc_lo_cc(q, n[j], t[i + j]);
-                t[i + j + 1] = madc_hi_cc(q, n[j], t[i + j + 1]);
-            }
-            pend = addc(c1, 0u);
-        }
+    for (int k = 0; k < 2 * L + 2; k++) {
+        E[k] = k < 2 * L + 1 ? t[k] : 0u;
+        F[k] = 0;
     }
-    t[2 * L] += pend;
-    // u = t[L .. 2L] < 2n; x = u - n if u >= n else u
-    uint32_t d[L];
-    d[0] = sub_cc(t[L], n[0]);
-#pragma unroll
-    for (int j = 1; j < L; j++) d[j] = subc_cc(t[L + j], n[j]);
-    const uint32_t top = subc(t[2 * L], 0u);  // 0 if u >= n, 0xffffffff on borrow
-    const bool keep = top != 0;
-#pragma unroll
-    for (int j = 0; j < L; j++) x[j] = keep ? t[L + j] : d[j];
+    mont_redc_ef<L>(E, F, n, ninv, x);
 }
 
-// x = x^2 * R^-1 mod n (x < n in and out).  Squaring by cross products,
-// doubling, and the diagonal squares, then REDC.
+// x = x^2 * R^-1 mod n (x < n in and out).  Cross products once, doubled,
+// diagonal squares added, then REDC.
 template <int L>
 __device__ __forceinline__ void mont_sqr(uint32_t (&x)[L], const uint32_t (&n)[L], uint32_t ninv) {
-    uint32_t t[2 * L + 1];
+    uint32_t E[2 * L + 2], F[2 * L + 2];
 #pragma unroll
-    for (int i = 0; i < 2 * L + 1; i++) t[i] = 0;
-    // cross products: row i adds x_i * x[i+1 .. L-1] at words 2i+1 .. i+L;
-    // the running sum stays below 2^(32(i+L+1)) so nothing leaves word i+L.
+    for (int k = 0; k < 2 * L + 2; k++) E[k] = F[k] = 0;
+    // cross products x_i * x_j (j > i) at position i + j, row i in two chains
+    // (j - i odd, j - i even).  Each array stays below B^(i+L+1) after row i,
+    // so a chain's carry out stops in the word above its top pair.
 #pragma unroll
     for (int i = 0; i < L - 1; i++) {
-        const int N = L - 1 - i;
-        const int off = 2 * i + 1;
         const uint32_t a = x[i];
-        // even chain: jj = 0, 2, ... (product a * x[i+1+jj]: lo at off+jj, hi at off+jj+1)
-        t[off] = mad_lo_cc(a, x[i + 1], t[off]);
-        if (N > 1) {
-            t[off + 1] = madc_hi_cc(a, x[i + 1], t[off + 1]);
 #pragma unroll
-            for (int jj = 2; jj < N; jj += 2) {
-                t[off + jj] = madc_lo_cc(a, x[i + 1 + jj], t[off + jj]);
-                if (jj + 1 < N || (N & 1) == 0)
-                    t[off + jj + 1] = madc_hi_cc(a, x[i + 1 + jj], t[off + jj + 1]);
-                else
-                    t[off + jj + 1] = madc_hi(a, x[i + 1 + jj], t[off + jj + 1]);  // ends at the top word
-            }
-            if ((N & 1) == 0) t[off + N] = addc(t[off + N], 0u);  // even chain ended at off+N-1
-            // odd chain: jj = 1, 3, ...
-            t[off + 1] = mad_lo_cc(a, x[i + 2], t[off + 1]);
+        for (int c = 0; c < 2; c++) {
+            const int j0 = i + 1 + c;
+            if (j0 >= L) continue;
+            int jl = j0;
 #pragma unroll
-            for (int jj = 1; jj < N; jj += 2) {
-                if (jj > 1) t[off + jj] = madc_lo_cc(a, x[i + 1 + jj], t[off + jj]);
-                if (jj + 2 < N || (N & 1) == 1)
-                    t[off + jj + 1] = madc_hi_cc(a, x[i + 1 + jj], t[off + jj + 1]);
-                else
-                    t[off + jj + 1] = madc_hi(a, x[i + 1 + jj], t[off + jj + 1]);  // ends at the top word
+            for (int j = j0; j < L; j += 2) jl = j;
+#pragma unroll
+            for (int j = j0; j < L; j += 2) {
+                const int p = i + j;
+                if ((p & 1) == 0) {
+                    if (j == j0) mad_link<true>(E[p], E[p + 1], a, x[j]);
+                    else mad_link<false>(E[p], E[p + 1], a, x[j]);
+                } else {
+                    if (j == j0) mad_link<true>(F[p - 1], F[p], a, x[j]);
+                    else mad_link<false>(F[p - 1], F[p], a, x[j]);
+                }
             }
-            if ((N & 1) == 1) t[off + N] = addc(t[off + N], 0u);  // odd chain ended at off+N-1
-        } else {
-            t[off + 1] = madc_hi(a, x[i + 1], t[off + 1]);  // single product, hi is the top word
+            const int cp = i + jl + 2;
+            if ((cp & 1) == 0)
+                E[cp] = addc(E[cp], 0u);
+            else
+                F[cp - 1] = addc(F[cp - 1], 0u);
         }
     }
-    // double (the cross sum is < 2^(64L-1), so no bit leaves word 2L-1)
+    // double both arrays (each holds less than half of B^(2L))
 #pragma unroll
-    for (int k = 2 * L - 1; k >= 1; k--) t[k] = __funnelshift_l(t[k - 1], t[k], 1);
-    t[0] = t[0] << 1;
-    // diagonal squares x_i^2 at words 2i, 2i+1, one carry chain
-    t[0] = mad_lo_cc(x[0], x[0], t[0]);
-    t[1] = madc_hi_cc(x[0], x[0], t[1]);
+    for (int k = 2 * L - 1; k >= 1; k--) E[k] = __funnelshift_l(E[k - 1], E[k], 1);
+    E[0] <<= 1;
+#pragma unroll
+    for (int k = 2 * L - 1; k >= 1; k--) F[k] = __funnelshift_l(F[k - 1], F[k], 1);
+    F[0] <<= 1;
+    // diagonal squares x_i^2 at the even positions 2i, one chain into E
+    mad_link<true>(E[0], E[1], x[0], x[0]);
 #pragma unroll
     for (int i = 1; i < L; i++) {
-        t[2 * i] = madc_lo_cc(x[i], x[i], t[2 * i]);
+        E[2 * i] = madc_lo_cc(x[i], x[i], E[2 * i]);
         if (i + 1 < L)
-            t[2 * i + 1] = madc_hi_cc(x[i], x[i], t[2 * i + 1]);
+            E[2 * i + 1] = madc_hi_cc(x[i], x[i], E[2 * i + 1]);
         else
-            t[2 * i + 1] = madc_hi(x[i], x[i], t[2 * i + 1]);
+            E[2 * i + 1] = madc_hi(x[i], x[i], E[2 * i + 1]);
     }
-    mont_redc<L>(t, n, ninv, x);
+    mont_redc_ef<L>(E, F, n, ninv, x);
 }
 
 // x = 2x mod n (x < n)

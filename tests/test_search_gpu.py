@@ -105,7 +105,7 @@ def test_odd_start_and_small_windows(pg, oracle):
             assert np.array_equal(res.prev_gap, prev) and np.array_equal(res.next_gap, nxt)
 
 
-@pytest.mark.parametrize("flags", [0, 1])  # 1 = PG_SUBMIT_DRAIN
+@pytest.mark.parametrize("flags", [0, 1, 6 << 16, (2 << 16) | (32 << 8) | 1])  # drain / warps-per-SM cap / both
 def test_pipelined_windows_equal_synchronous(pg, flags):
     windows = [(1_000_000, 20_000), (1_020_000, 20_000), (1_040_000, 7_001), (1_000_000, 20_000)]
     with pg.Job(503, 2190, 10_000, 50_000_000, max_m_inc=20_000, max_m=2_000_000) as job:
