@@ -10,6 +10,8 @@
 //   --ranges R    windows of --minc m to search; 0 = until Ctrl-C (the reference's only mode)
 //   --chunk C     m per device call (default min(minc, 1,000,000))
 //   --form persistent|plain   --rounds R   --device N
+//   --warps-per-sm W   cap on each window's PRP warps per SM (default 6; 0 = all that fit):
+//                      two windows are in flight and share the SMs
 // Record lines "{gap} {merit:.3f} {m} * {P}# / {D} - {prev}" go to stdout and
 // are appended to records_{P}.txt.  Ctrl-C once: finish the current window;
 // twice: stop after the current device call; three times: exit(2)
@@ -47,6 +49,7 @@ struct Config {
     int form = PG_SEARCH_PERSISTENT;
     uint32_t rounds = 1;
     int device = 0;
+    uint32_t warps_per_sm = 6;
 };
 
 static void show_usage(const char *name) {
@@ -58,7 +61,9 @@ static void show_usage(const char *name) {
     printf("  --sl <X>        sieve X in [-sl, sl] around m*K (default 8*ln(m*K))\n");
     printf("  --ranges <R>    search R windows of minc m, 0 = until Ctrl-C (default 0)\n");
     printf("  --chunk <C>     m per device call (default min(minc, 1000000))\n");
-    printf("  --form persistent|plain   --rounds <bases>   --device <n>\n\n");
+    printf("  --form persistent|plain   --rounds <bases>   --device <n>\n");
+    printf("  --warps-per-sm <W>  PRP warps per SM of each of the two windows in flight\n");
+    printf("                      (default 6, 0 = as many as fit)\n\n");
     printf("[OPTIONAL]\n  -q, --quiet\n  -v, --verbose\n  -h, --help\n");
 }
 
@@ -79,6 +84,7 @@ static Config argparse(int argc, char **argv) {
         {"sl", required_argument, 0, 20},         {"ranges", required_argument, 0, 21},
         {"chunk", required_argument, 0, 22},      {"form", required_argument, 0, 23},
         {"rounds", required_argument, 0, 24},     {"device", required_argument, 0, 25},
+        {"warps-per-sm", required_argument, 0, 26},
         {"quiet", no_argument, 0, 'q'},           {"verbose", no_argument, 0, 'v'},
         {"help", no_argument, 0, 'h'},            {0, 0, 0, 0}};
     Config c;
@@ -108,6 +114,7 @@ static Config argparse(int argc, char **argv) {
                 break;
             case 24: c.rounds = (uint32_t)atoi(optarg); break;
             case 25: c.device = atoi(optarg); break;
+            case 26: c.warps_per_sm = (uint32_t)atoi(optarg); break;
             default: c.valid = 0;
         }
     }
@@ -198,34 +205,61 @@ int main(int argc, char **argv) {
     char fname[64];
     snprintf(fname, sizeof fname, "records_%u.txt", c.p);
     FILE *rec = fopen(fname, "a");
-    std::vector<uint64_t> ms(chunk);
-    std::vector<uint32_t> prev(chunk), next(chunk);
+    // PG_SEARCH_SLOTS windows in flight: while one window's gaps are read and
+    // its records written, the next window runs on the device
+    struct Pending {
+        uint64_t ticket;
+        int buf;
+    };
+    std::vector<uint64_t> ms[PG_SEARCH_SLOTS];
+    std::vector<uint32_t> prev[PG_SEARCH_SLOTS], next[PG_SEARCH_SLOTS];
+    for (int k = 0; k < PG_SEARCH_SLOTS; k++) {
+        ms[k].resize(chunk);
+        prev[k].resize(chunk);
+        next[k].resize(chunk);
+    }
+    const uint32_t flags = c.form == PG_SEARCH_PERSISTENT ? PG_SUBMIT_WARPS_PER_SM(c.warps_per_sm) : 0u;
+    std::vector<Pending> pending;
     uint64_t total_m = 0, total_tests = 0, total_primes = 0, total_ext = 0;
     const auto t0 = std::chrono::steady_clock::now();
-    uint64_t m_start = c.m_start;
-    for (uint64_t r = 0; (c.ranges == 0 || r < c.ranges) && g_stop == 0; r++) {
-        for (uint64_t off = 0; off < c.m_inc && g_stop < 2; off += chunk) {
-            const uint64_t inc = std::min(chunk, c.m_inc - off);
-            pg_search_stats st{};
-            CHECK(pg_search(job, m_start + off, inc, c.form, ms.data(), prev.data(), next.data(), &st));
-            total_m += st.m_count;
-            total_tests += st.prp_tests;
-            total_primes += 2 * st.m_count;
-            total_ext += st.extended_sides;
-            for (uint64_t i = 0; i < st.m_count; i++) {
-                const uint64_t gap = (uint64_t)prev[i] + next[i];
-                const double merit = pg_merit(info.k_log, ms[i], gap);
-                if (merit > c.min_merit) {
-                    char line[160];
-                    pg_format_record(line, sizeof line, gap, merit, ms[i], c.p, c.d, prev[i]);
-                    printf("%s\n", line);
-                    if (rec) {
-                        fprintf(rec, "%s\n", line);
-                        fflush(rec);
-                    }
+    auto finish_one = [&]() {
+        const Pending pd = pending.front();
+        pending.erase(pending.begin());
+        pg_search_stats st{};
+        CHECK(pg_search_wait(job, pd.ticket, ms[pd.buf].data(), prev[pd.buf].data(), next[pd.buf].data(), &st));
+        total_m += st.m_count;
+        total_tests += st.prp_tests;
+        total_primes += 2 * st.m_count;
+        total_ext += st.extended_sides;
+        for (uint64_t i = 0; i < st.m_count; i++) {
+            const uint64_t gap = (uint64_t)prev[pd.buf][i] + next[pd.buf][i];
+            const double merit = pg_merit(info.k_log, ms[pd.buf][i], gap);
+            if (merit > c.min_merit) {
+                char line[160];
+                pg_format_record(line, sizeof line, gap, merit, ms[pd.buf][i], c.p, c.d, prev[pd.buf][i]);
+                printf("%s\n", line);
+                if (rec) {
+                    fprintf(rec, "%s\n", line);
+                    fflush(rec);
                 }
             }
         }
+        return 0;
+    };
+    uint64_t m_start = c.m_start;
+    int next_buf = 0;
+    for (uint64_t r = 0; (c.ranges == 0 || r < c.ranges) && g_stop == 0; r++) {
+        for (uint64_t off = 0; off < c.m_inc && g_stop < 2; off += chunk) {
+            const uint64_t inc = std::min(chunk, c.m_inc - off);
+            if ((int)pending.size() == PG_SEARCH_SLOTS && finish_one()) return 1;
+            uint64_t ticket = 0;
+            CHECK(pg_search_submit(job, m_start + off, inc, c.form, flags, &ticket));
+            pending.push_back({ticket, next_buf});
+            next_buf = (next_buf + 1) % PG_SEARCH_SLOTS;
+        }
+        // the range's last windows finish before its summary
+        while (!pending.empty())
+            if (finish_one()) return 1;
         m_start += c.m_inc;
         if (c.verbose >= 1) {
             const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

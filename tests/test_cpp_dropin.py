@@ -44,13 +44,16 @@ def test_dropin_results(pg, tmp_path):
 
 
 @pytest.mark.gpu
-def test_cli_records(pg, tmp_path):
-    """gap_search_gpu on the P=337 window prints the GMP records of merit > 5."""
+@pytest.mark.parametrize("extra", [[], ["--chunk", "1500"], ["--chunk", "1500", "--warps-per-sm", "0"],
+                                   ["--chunk", "2500", "--form", "plain"]])
+def test_cli_records(pg, tmp_path, extra):
+    """gap_search_gpu on the P=337 window prints the GMP records of merit > 5, in m order, also when the
+    range is cut into chunks that run two at a time."""
     from conftest import golden
     g = golden("gaps_cfg1.json")
     cli = pg.LIB_PATH.parent / "gap_search_gpu"
     out = subprocess.run([str(cli), "-p", "337", "-d", "2310", "--mstart", "10000000", "--minc", "10000",
-                          "--max-prime", "100", "--min-merit", "5", "--sl", "7500", "--ranges", "1", "-q"],
+                          "--max-prime", "100", "--min-merit", "5", "--sl", "7500", "--ranges", "1", "-q", *extra],
                          capture_output=True, text=True, cwd=tmp_path, check=True).stdout
     import re
     rec = re.compile(r"^\d+ \d+\.\d{3} \d+ \* \d+# / \d+ - \d+$")
