@@ -5,13 +5,13 @@
 // 136 words).  Lane g of a group holds words [g*LT, (g+1)*LT) of every value.
 // Multiplication is CIOS, row by row: the row's word of `a` is broadcast by a
 // warp shuffle, every lane multiplies its slice, lane 0 of the group derives
-// the Montgomery factor q and broadcasts it, and the accumulator shifts down
-// one word by a shuffle.  A carry leaving a lane's slice is not passed on at
-// once: it waits as that lane's pending "spill" (it belongs to the next
-// lane's lowest word) and is folded in when the shift brings that word down,
-// so a row has no serial carry chain across lanes.  Carries that remain at
-// the end are resolved in one step by carry lookahead over warp ballots
-// (generate / propagate bits per lane, added as integers).
+// the Montgomery factor q and broadcasts it, and each lane hands the word
+// leaving its bottom to the lane below.  Carries leaving a lane's slice are
+// not passed on at once: they stay in the top words of the lane's window
+// (they belong to the next lane's lowest words), so a row has no serial carry
+// chain across lanes.  What remains at the end is resolved in one step by
+// carry lookahead over warp ballots (generate / propagate bits per lane,
+// added as integers).
 //
 // Every shuffle and ballot names only the group's lanes, so the groups of a
 // warp may diverge (one idle, another still squaring).
@@ -119,7 +119,8 @@ __device__ __forceinline__ bool group_eq(const uint32_t (&x)[LT], const uint32_t
 }
 
 // acc (slice) + spill += ai * b (slice): lo products chain over the slice, hi
-// products one word up; what leaves the slice is added to the spill.
+// products one word up; what leaves the slice is added to the spill.  One row
+// only (building a candidate m*K), so the two chains are left unfused.
 template <int LT>
 __device__ __forceinline__ void row_mac(uint32_t (&acc)[LT], uint64_t &spill, uint32_t ai, const uint32_t (&b)[LT]) {
     acc[0] = mad_lo_cc(ai, b[0], acc[0]);
@@ -138,38 +139,119 @@ __device__ __forceinline__ void row_mac(uint32_t (&acc)[LT], uint64_t &spill, ui
     spill += h;
 }
 
-// r = a * b * R^-1 mod n, inputs and output in [0, 2n), 4n < R
+// Products m*v[k] of one row, k < LT, added at positions S + k of the lane's
+// window (S is a constant once the caller's row loop is unrolled): products
+// whose low word lands at an even position go to E (pairs E[P], E[P+1]), at an
+// odd position to H (pairs H[P], H[P+1]), so every link is one fused
+// multiply-add on an aligned register pair.  Each chain's carry out is added
+// two words up (the top words only gather carries and cannot overflow).
+template <int LT, int PH>
+__device__ __forceinline__ void gmac_row(uint32_t (&E)[PH], uint32_t (&H)[PH], int S, uint32_t m,
+                                         const uint32_t (&v)[LT]) {
+#pragma unroll
+    for (int par = 0; par < 2; par++) {  // par 0: even positions (E), 1: odd (H)
+        const int k0 = ((S & 1) == par) ? 0 : 1;
+        if (k0 >= LT) continue;
+        const int kl = k0 + ((LT - 1 - k0) / 2) * 2;
+#pragma unroll
+        for (int k = k0; k < LT; k += 2) {
+            const int P = S + k;
+            if (par == 0) {
+                if (k == k0) mad_link<true>(E[P], E[P + 1], m, v[k]);
+                else mad_link<false>(E[P], E[P + 1], m, v[k]);
+            } else {
+                if (k == k0) mad_link<true>(H[P], H[P + 1], m, v[k]);
+                else mad_link<false>(H[P], H[P + 1], m, v[k]);
+            }
+        }
+        const int C = S + kl + 2;
+        if (par == 0) {
+            E[C] = addc_cc(E[C], 0u);
+            E[C + 1] = addc(E[C + 1], 0u);
+        } else {
+            H[C] = addc_cc(H[C], 0u);
+            H[C + 1] = addc(H[C + 1], 0u);
+        }
+    }
+}
+
+// r = a * b * R^-1 mod n, inputs and output in [0, 2n), 4n < R.  CIOS, row by
+// row: the row's word of a is broadcast by a shuffle, every lane multiplies
+// its slice, lane 0 derives the Montgomery factor q and broadcasts it.  The
+// accumulator is kept as two arrays (E, H) in a window that moves up one word
+// per row instead of being shifted down (a shift would change the register
+// pairing of every word and cost moves on every product): row w
+// of a source lane's LT rows works at offset w, so every index is a
+// compile-time constant and every product is one fused 64-bit multiply-add;
+// after the LT rows the window is moved back by LT words.  A lane sends the
+// word leaving its bottom (E + H, up to 33 bits) to the lane below, which adds
+// it LT words up; in lane 0 that word is 0 mod 2^32 (the Montgomery step) and
+// only its carry stays, in c0, for the next bottom word.
 template <int T, int LT>
 __device__ __forceinline__ void gmont_mul(const Group<T> &G, uint32_t (&r)[LT], const uint32_t (&a)[LT],
-                                          const uint32_t (&b)[LT], const uint32_t (&n)[LT], uint32_t ninv) {
-    uint32_t acc[LT];
+                                           const uint32_t (&b)[LT], const uint32_t (&n)[LT], uint32_t ninv) {
+    constexpr int PH = 2 * LT + 4;
+    uint32_t E[PH], H[PH];
 #pragma unroll
-    for (int k = 0; k < LT; k++) acc[k] = 0;
-    uint64_t spill = 0;
+    for (int k = 0; k < PH; k++) E[k] = H[k] = 0;
+    uint32_t c0 = 0;  // lane 0: carry into the bottom word
+    const bool bottom = G.gl == 0, top = G.gl == T - 1;
+#pragma unroll 1
     for (int src = 0; src < T; src++) {
 #pragma unroll
         for (int w = 0; w < LT; w++) {
             const uint32_t ai = __shfl_sync(G.gmask, a[w], G.gb + src);
-            row_mac<LT>(acc, spill, ai, b);
-            uint32_t q = acc[0] * ninv;  // meaningful in the group's lane 0
-            q = __shfl_sync(G.gmask, q, G.gb);
-            row_mac<LT>(acc, spill, q, n);
-            // shift down one word: this slice's lowest word is 0 in lane 0 and
-            // moves to the previous lane elsewhere; the next lane's lowest word
-            // (plus this lane's spill, which belongs to that position) arrives on top
-            uint32_t nxt = __shfl_down_sync(G.gmask, acc[0], 1);
-            if (G.gl == T - 1) nxt = 0;
+            gmac_row<LT, PH>(E, H, w, ai, b);
+            // Montgomery factor from lane 0's bottom word
+            uint32_t q = add_cc(E[w], H[w]);
+            q = add_cc(q, c0);
+            q = __shfl_sync(G.gmask, q * ninv, G.gb);
+            gmac_row<LT, PH>(E, H, w, q, n);
+            // the bottom word leaves: 0 mod 2^32 in lane 0 (its carry stays),
+            // handed to the lane below elsewhere
+            uint32_t lo = add_cc(E[w], H[w]);
+            uint32_t hi = addc(0u, 0u);
+            if (bottom) {
+                (void)add_cc(lo, c0);
+                c0 = addc(hi, 0u);
+            }
+            uint32_t rlo = __shfl_down_sync(G.gmask, lo, 1);
+            uint32_t rhi = __shfl_down_sync(G.gmask, hi, 1);
+            if (top) rlo = rhi = 0;
+            const int P = w + LT;
+            if ((P & 1) == 0) {
+                E[P] = add_cc(E[P], rlo);
+                E[P + 1] = addc_cc(E[P + 1], rhi);
+                E[P + 2] = addc(E[P + 2], 0u);
+            } else {
+                H[P] = add_cc(H[P], rlo);
+                H[P + 1] = addc_cc(H[P + 1], rhi);
+                H[P + 2] = addc(H[P + 2], 0u);
+            }
+        }
+        // move the window back by LT words
 #pragma unroll
-            for (int k = 0; k < LT - 1; k++) acc[k] = acc[k + 1];
-            const uint64_t v = (uint64_t)nxt + spill;
-            acc[LT - 1] = (uint32_t)v;
-            spill = v >> 32;
+        for (int k = 0; k < PH; k++) {
+            E[k] = k + LT < PH ? E[k + LT] : 0u;
+            H[k] = k + LT < PH ? H[k + LT] : 0u;
         }
     }
-    // fold each spill into the next lane's lowest word and resolve the carries
-    const uint32_t lo = __shfl_up_sync(G.gmask, (uint32_t)spill, 1);
-    const uint32_t hi = __shfl_up_sync(G.gmask, (uint32_t)(spill >> 32), 1);
-    const uint64_t in = (G.gl == 0) ? 0ull : ((uint64_t)hi << 32 | lo);
+    // the slice (positions 0 .. LT-1) and what lies above it (LT, LT+1), plus
+    // lane 0's last carry at position 0
+    uint32_t R[LT + 2];
+    R[0] = add_cc(E[0], H[0]);
+#pragma unroll
+    for (int k = 1; k < LT + 2; k++) R[k] = (k + 1 < LT + 2) ? addc_cc(E[k], H[k]) : addc(E[k], H[k]);
+    R[0] = add_cc(R[0], bottom ? c0 : 0u);
+#pragma unroll
+    for (int k = 1; k < LT + 2; k++) R[k] = (k + 1 < LT + 2) ? addc_cc(R[k], 0u) : addc(R[k], 0u);
+    const uint64_t spill = ((uint64_t)R[LT + 1] << 32) | R[LT];
+    const uint32_t slo = __shfl_up_sync(G.gmask, (uint32_t)spill, 1);
+    const uint32_t shi = __shfl_up_sync(G.gmask, (uint32_t)(spill >> 32), 1);
+    const uint64_t in = bottom ? 0ull : ((uint64_t)shi << 32 | slo);
+    uint32_t acc[LT];
+#pragma unroll
+    for (int k = 0; k < LT; k++) acc[k] = R[k];
     resolve_in<T, LT>(G, acc, in);
 #pragma unroll
     for (int k = 0; k < LT; k++) r[k] = acc[k];
