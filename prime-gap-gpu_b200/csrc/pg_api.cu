@@ -395,6 +395,31 @@ static int tables_build(pg::Tables &T, const pg_job_params &p, cudaStream_t st) 
         if (e == cudaSuccess)
             e = launch_prime_tables(d_K, (uint32_t)T.K.size(), T.np, T.d_lp, T.d_lc, T.d_lcinv, T.wide, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        // order each segment's primes by the modular search's Euclid depth (the
+        // table is used unordered if the extra copy does not fit)
+        if (e == cudaSuccess) {
+            uint8_t *op = nullptr, *oc = nullptr, *oci = nullptr, *dep = nullptr;
+            uint64_t extra = 0;
+            if (!dalloc(extra, &op, acc * esz) && !dalloc(extra, &oc, acc * esz) && !dalloc(extra, &oci, acc * esz) &&
+                !dalloc(extra, &dep, acc)) {
+                e = launch_prime_reorder(acc, nseg, d_off, T.d_lp, T.d_lc, T.d_lcinv, op, oc, oci, dep, T.wide, st);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+                if (e == cudaSuccess) {  // keep the ordered copies, free the others below
+                    void *old[3] = {T.d_lp, T.d_lc, T.d_lcinv};
+                    T.d_lp = op;
+                    T.d_lc = oc;
+                    T.d_lcinv = oci;
+                    op = (uint8_t *)old[0];
+                    oc = (uint8_t *)old[1];
+                    oci = (uint8_t *)old[2];
+                }
+            }
+            g_last_error.clear();
+            cudaFree(op);  // the unordered copies (or the unused new ones)
+            cudaFree(oc);
+            cudaFree(oci);
+            cudaFree(dep);
+        }
         free_scratch();
         if (e != cudaSuccess) return fail(PG_ERR_CUDA, "prime tables: %s", cudaGetErrorString(e));
     }

@@ -115,6 +115,11 @@ cudaError_t launch_prime_write(uint64_t v_first, uint64_t limit, const uint32_t 
                                uint32_t nseg, const uint64_t *seg_offsets, void *out, bool wide, cudaStream_t st);
 cudaError_t launch_prime_tables(const uint32_t *K, uint32_t kwords, uint64_t np, const void *p, void *c,
                                 void *cinv, bool wide, cudaStream_t st);
+// orders the primes of every segment by the modular search's Euclid depth
+// (into op / oc / oci; depth: np bytes of scratch)
+cudaError_t launch_prime_reorder(uint64_t np, uint32_t nseg, const uint64_t *seg_off, const void *p, const void *c,
+                                 const void *ci, void *op, void *oc, void *oci, uint8_t *depth, bool wide,
+                                 cudaStream_t st);
 cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, cudaStream_t st);
 cudaError_t launch_sieve_small(const SieveArgs &a, bool compact, cudaStream_t st);
 cudaError_t launch_prp_batch(uint32_t L, const uint32_t *cand, uint32_t words, uint32_t n, uint32_t rounds,

@@ -203,6 +203,82 @@ cudaError_t launch_prime_tables(const uint32_t *K, uint32_t kwords, uint64_t np,
     return cudaGetLastError();
 }
 
+// ========================================================= depth ordering
+
+// The modular search's Euclid depth for a prime depends on p and K mod p
+// (and on the window width), not on the window.  Ordering the primes of each
+// sieve segment by that depth gives the threads of a warp equal trip counts;
+// segments keep their order, so prime-table indices of segment boundaries
+// still split the table by value.
+constexpr uint32_t DEPTH_W = 8192;  // reference window width (2 * sly) for the ordering
+constexpr int DEPTH_BINS = 64;
+
+template <typename T>
+__global__ void k_prime_depth(uint64_t np, const T *p, const T *c, uint8_t *depth) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    uint64_t M = p[i], A = M - c[i];  // A = -K mod p, c in [1, p)
+    int d = 0;
+    while (A > DEPTH_W + 1 && d < DEPTH_BINS - 1) {
+        const uint64_t r = M % A;
+        M = A;
+        A = r;
+        d++;
+    }
+    depth[i] = (uint8_t)d;
+}
+
+// One block per segment: counting sort of the segment's primes by depth.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_prime_reorder(const uint64_t *seg_off, uint32_t nseg, uint64_t np,
+                                                        const uint8_t *depth, const T *p, const T *c, const T *ci,
+                                                        T *op, T *oc, T *oci) {
+    __shared__ uint32_t hist[DEPTH_BINS];
+    const uint64_t lo = seg_off[blockIdx.x];
+    const uint64_t hi = blockIdx.x + 1 < nseg ? seg_off[blockIdx.x + 1] : np;
+    if (threadIdx.x < DEPTH_BINS) hist[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) atomicAdd(&hist[depth[i]], 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int b = 0; b < DEPTH_BINS; b++) {
+            const uint32_t v = hist[b];
+            hist[b] = acc;
+            acc += v;
+        }
+    }
+    __syncthreads();
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        const uint64_t pos = lo + atomicAdd(&hist[depth[i]], 1u);
+        op[pos] = p[i];
+        oc[pos] = c[i];
+        oci[pos] = ci[i];
+    }
+}
+
+cudaError_t launch_prime_reorder(uint64_t np, uint32_t nseg, const uint64_t *seg_off, const void *p, const void *c,
+                                 const void *ci, void *op, void *oc, void *oci, uint8_t *depth, bool wide,
+                                 cudaStream_t st) {
+    if (np == 0 || nseg == 0) return cudaSuccess;
+    const uint32_t threads = 256;
+    const uint64_t blocks = (np + threads - 1) / threads;
+    if (wide) {
+        k_prime_depth<uint64_t><<<(unsigned)blocks, threads, 0, st>>>(np, (const uint64_t *)p, (const uint64_t *)c,
+                                                                      depth);
+        k_prime_reorder<uint64_t><<<nseg, 1024, 0, st>>>(seg_off, nseg, np, depth, (const uint64_t *)p,
+                                                         (const uint64_t *)c, (const uint64_t *)ci, (uint64_t *)op,
+                                                         (uint64_t *)oc, (uint64_t *)oci);
+    } else {
+        k_prime_depth<uint32_t><<<(unsigned)blocks, threads, 0, st>>>(np, (const uint32_t *)p, (const uint32_t *)c,
+                                                                      depth);
+        k_prime_reorder<uint32_t><<<nseg, 1024, 0, st>>>(seg_off, nseg, np, depth, (const uint32_t *)p,
+                                                         (const uint32_t *)c, (const uint32_t *)ci, (uint32_t *)op,
+                                                         (uint32_t *)oc, (uint32_t *)oci);
+    }
+    return cudaGetLastError();
+}
+
 // ====================================================== large-prime sieve
 
 __device__ __forceinline__ void mark_hit(const LargeArgs &a, uint64_t j, uint32_t idx) {
