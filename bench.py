@@ -381,7 +381,7 @@ def run_serve(args) -> dict:
     reqs = serve_requests(args.serve_jobs)
     classes = sorted({(p, d) for p, d, *_ in reqs})
     max_sl = max(r[2] for r in reqs)
-    with pg.Server(0, max_sl=max_sl, warps_per_sm=args.warps_per_sm) as srv:
+    with pg.Server(0, max_sl=max_sl, warps_per_sm=args.warps_per_sm, batch_m=args.serve_batch_m) as srv:
         # resident tables for every (P, d) first: one small request per class
         warm = [srv.submit(p, d, 1_000, reqs[0][3], 1_000_001, 200) for p, d in classes]
         t = time.perf_counter()
@@ -396,8 +396,8 @@ def run_serve(args) -> dict:
         m_total = sum(x["m_count"] for x in infos)
         cap_jobs = len(reqs) / span
         st_closed = srv.stats()
-        # open loop: Poisson arrivals at 70% of capacity
-        rate = 0.7 * cap_jobs
+        # open loop: Poisson arrivals at 70% of capacity (or at the given rate)
+        rate = args.serve_rate if args.serve_rate > 0 else 0.7 * cap_jobs
         gaps = np.random.default_rng(SERVE_SEED + 1).exponential(1.0 / rate, len(reqs))
         arrivals = np.cumsum(gaps)
         ids2 = [None] * len(reqs)
@@ -429,7 +429,8 @@ def run_serve(args) -> dict:
         "n_gpus": 1, "data": "synthetic (seeded request mix)",
         "config": {"workload": f"{len(reqs)} requests, P in {{337,503,907}}, d in {{210,2190,2310}}, "
                                "500-20000 m from [1e6,1e9], SL=round(8 ln N), primes <= 1e9",
-                   "seed": SERVE_SEED, "warps_per_sm": args.warps_per_sm},
+                   "seed": SERVE_SEED, "warps_per_sm": args.warps_per_sm,
+                   "batch_m": args.serve_batch_m or 65536},
     }
 
 
@@ -454,6 +455,10 @@ def main(argv=None) -> int:
     ap.add_argument("--serve", action="store_true",
                     help="the serving workload instead: p50/p99 latency of a request mix (pg_server_*)")
     ap.add_argument("--serve-jobs", type=int, default=256)
+    ap.add_argument("--serve-batch-m", type=int, default=0,
+                    help="coprime m per search launch of the server (0 = its default, 65536)")
+    ap.add_argument("--serve-rate", type=float, default=0.0,
+                    help="arrival rate in requests/s for the latency run (0 = 70%% of the measured capacity)")
     args = ap.parse_args(argv)
     if args.warps_per_sm is None:
         args.warps_per_sm = 0 if args.serve else 6
