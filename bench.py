@@ -6,8 +6,8 @@ N = m*503#/2190 + X for X in [-10,000, 10,000] sieved by every prime <= 2e9,
 strong base-2 PRP outward from X = 0 for the previous and the next prime,
 records of merit > 22.  A step is one search of that window (sieve + PRP +
 finalize), the inputs being the window bounds; the prime tables (98 M primes,
-786 MB with their K^-1 residues) are read again by every step, far more than
-the 126 MB L2, so no L2 flush is needed between steps.
+1.18 GB with their K mod p and K^-1 residues) are read again by every step, far
+more than the 126 MB L2, so no L2 flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -298,7 +298,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
                            + (f", draining to {args.drain} lanes per unresolved side" if args.drain else ""),
                    "m_per_gpu_per_step": m_count, "sl": W["sl"], "max_prime": W["max_prime"],
                    "limbs": job.info["limbs"], "parallelism": f"weak: {world} disjoint m-windows",
-                   "l2": "inputs larger than L2 (786 MB prime tables read every step)"},
+                   "l2": "inputs larger than L2 (1.18 GB prime tables read every step)"},
         "prp_tests_per_sec": sum(r["tests"] for r in allr) / dev_s,
         "ms_per_step_one_window_alone": max(r["sync_ms"] for r in allr),
         "setup_seconds": setup_s,
