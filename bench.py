@@ -381,7 +381,8 @@ def run_serve(args) -> dict:
     reqs = serve_requests(args.serve_jobs)
     classes = sorted({(p, d) for p, d, *_ in reqs})
     max_sl = max(r[2] for r in reqs)
-    with pg.Server(0, max_sl=max_sl, warps_per_sm=args.warps_per_sm, batch_m=args.serve_batch_m) as srv:
+    with pg.Server(0, max_sl=max_sl, warps_per_sm=args.warps_per_sm, batch_m=args.serve_batch_m,
+                   slots=args.serve_slots) as srv:
         # resident tables for every (P, d) first: one small request per class
         warm = [srv.submit(p, d, 1_000, reqs[0][3], 1_000_001, 200) for p, d in classes]
         t = time.perf_counter()
@@ -430,7 +431,7 @@ def run_serve(args) -> dict:
         "config": {"workload": f"{len(reqs)} requests, P in {{337,503,907}}, d in {{210,2190,2310}}, "
                                "500-20000 m from [1e6,1e9], SL=round(8 ln N), primes <= 1e9",
                    "seed": SERVE_SEED, "warps_per_sm": args.warps_per_sm,
-                   "batch_m": args.serve_batch_m or 65536},
+                   "batch_m": args.serve_batch_m or 65536, "slots": args.serve_slots or 2},
     }
 
 
@@ -457,6 +458,7 @@ def main(argv=None) -> int:
     ap.add_argument("--serve-jobs", type=int, default=256)
     ap.add_argument("--serve-batch-m", type=int, default=0,
                     help="coprime m per search launch of the server (0 = its default, 65536)")
+    ap.add_argument("--serve-slots", type=int, default=0, help="server launch slots (0 = its default, 2)")
     ap.add_argument("--serve-rate", type=float, default=0.0,
                     help="arrival rate in requests/s for the latency run (0 = 70%% of the measured capacity)")
     args = ap.parse_args(argv)

@@ -269,7 +269,9 @@ typedef struct {
     uint32_t ext_window;   /* as pg_job_params (0 = default) */
     uint32_t tpi;          /* as pg_job_params (0 = automatic) */
     uint32_t warps_per_sm; /* cap on each launch's PRP warps per SM (PG_SUBMIT_WARPS_PER_SM), so the
-                              two launches in flight share the SMs; 0 = as many as fit */
+                              launches in flight share the SMs; 0 = as many as fit */
+    uint32_t slots;        /* launches in flight (own stream and buffers each); 0 = 2, at most 8 */
+    uint32_t pad;
 } pg_server_params;
 
 typedef struct {

@@ -18,9 +18,10 @@
 //      side's constants from its window's WinInfo.
 //   3. finish the oldest launch in flight and scatter its gaps to the
 //      requests; a request is done when its last window is.
-// Two slots keep one launch queued behind the running one, so the host work
-// of step 2 overlaps the device; the worker polls the running launch's stream
-// so requests that arrive meanwhile go into the other slot at once.
+// Two slots (pg_server_params.slots) keep one launch queued behind the running
+// one, so the host work of step 2 overlaps the device; the worker polls the
+// running launch's stream so requests that arrive meanwhile go into a free
+// slot at once.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -40,8 +41,6 @@
 using namespace pg;
 
 namespace {
-
-constexpr int NSLOTS = 2;
 
 struct TableKey {
     uint32_t p, d, q1;
@@ -126,7 +125,7 @@ struct pg_server {
     std::deque<uint64_t> done_ids;      // finished, not yet returned by next_done
     std::map<TableKey, TableEntry> tables;
     uint64_t admissions = 0;
-    SlotState slot[NSLOTS];
+    std::vector<SlotState> slot;  // launch slots (pg_server_params.slots)
     uint64_t slot_bytes = 0;
     uint64_t launch_seq = 0;
     pg_server_stats st{};
@@ -444,6 +443,8 @@ extern "C" int pg_server_create(int device, const pg_server_params *params, pg_s
     if (!p.ext_window) p.ext_window = 64;
     if (p.max_windows > 65535) return fail(PG_ERR_ARG, "max_windows=%u > 65535", p.max_windows);
     if (p.max_sl / 2 > 65535) return fail(PG_ERR_ARG, "max_sl=%u > 131071", p.max_sl);
+    if (!p.slots) p.slots = 2;
+    if (p.slots > 8) return fail(PG_ERR_ARG, "slots=%u > 8", p.slots);
     pg_ctx *c = nullptr;
     int rc = pg_ctx_create(device, &c);
     if (rc) return rc;
@@ -456,6 +457,7 @@ extern "C" int pg_server_create(int device, const pg_server_params *params, pg_s
     srv->ctx = c;
     srv->prm = p;
     srv->t0 = std::chrono::steady_clock::now();
+    srv->slot.resize(p.slots);
     // launch capacities: batch_m coprime m over at most max_windows windows
     // of window_m m; lists at most half of each side's positions
     const uint64_t nodd_w = p.window_m / 2 + 1;
