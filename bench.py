@@ -261,7 +261,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
     # bit-exactness self-check of this run against the committed GMP fixture
     exact = None
     if rank == 0:
-        gold = json.loads((ROOT / "tests" / "golden" / "gaps_cfg2.json").read_text())
+        gold = json.loads((ROOT / "tests" / "golden" / "gaps_P503_d2190.json").read_text())
         pos = {int(m): i for i, m in enumerate(res.ms)}
         exact = all((int(res.prev_gap[pos[m]]), int(res.next_gap[pos[m]])) == (a, b)
                     for m, a, b in zip(gold["ms"], gold["prev_gap"], gold["next_gap"]) if m in pos)

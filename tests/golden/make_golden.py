@@ -14,7 +14,7 @@ sympy, an independent implementation.
                      single- and multi-word)
   sieve_rows.json    sha256 of every sieve row of a P=337, d=2310 window,
                      plus a few full rows
-  gaps_cfg*.json     prev/next gaps from GMP for all m of the P=337 window
+  gaps_P*_d*.json    prev/next gaps from GMP for all m of the P=337 window
                      and seeded samples of the P=503, P=907 and P=3001 ones,
                      with the record lines above a merit threshold
 """
@@ -140,13 +140,13 @@ def main():
     print("prp vectors done", flush=True)
     (OUT / "sieve_rows.json").write_text(json.dumps(sieve_rows()))
     print("sieve rows done", flush=True)
-    cfgs = [
-        ("gaps_cfg1.json", "P=337 d=2310 full window", 337, 2310, 10_000_000, 10_000, 7_500, 100_000_000, None, 5.0),
-        ("gaps_cfg2.json", "P=503 d=2190 sample", 503, 2190, 1_000_000, 200_000, 10_000, 2_000_000_000, 48, 5.0),
-        ("gaps_cfg3.json", "P=907 d=210 sample", 907, 210, 1_000_000, 50_000, 18_000, 10_000_000_000, 24, 5.0),
-        ("gaps_cfg5.json", "P=3001 d=2190 sample", 3001, 2190, 1, 100_000, 40_000, 10_000_000_000, 6, 5.0),
+    windows = [
+        ("gaps_P337_d2310.json", "P=337 d=2310 full window", 337, 2310, 10_000_000, 10_000, 7_500, 100_000_000, None, 5.0),
+        ("gaps_P503_d2190.json", "P=503 d=2190 sample", 503, 2190, 1_000_000, 200_000, 10_000, 2_000_000_000, 48, 5.0),
+        ("gaps_P907_d210.json", "P=907 d=210 sample", 907, 210, 1_000_000, 50_000, 18_000, 10_000_000_000, 24, 5.0),
+        ("gaps_P3001_d2190.json", "P=3001 d=2190 sample", 3001, 2190, 1, 100_000, 40_000, 10_000_000_000, 6, 5.0),
     ]
-    for fname, name, P, d, ms, mi, sl, lim, sample, mm in cfgs:
+    for fname, name, P, d, ms, mi, sl, lim, sample, mm in windows:
         (OUT / fname).write_text(json.dumps(gaps(name, P, d, ms, mi, sl, lim, sample, mm, rng)))
         print(fname, "done", flush=True)
 

@@ -50,7 +50,7 @@ def test_cli_records(pg, tmp_path, extra):
     """gap_search_gpu on the P=337 window prints the GMP records of merit > 5, in m order, also when the
     range is cut into chunks that run two at a time."""
     from conftest import golden
-    g = golden("gaps_cfg1.json")
+    g = golden("gaps_P337_d2310.json")
     cli = pg.LIB_PATH.parent / "gap_search_gpu"
     out = subprocess.run([str(cli), "-p", "337", "-d", "2310", "--mstart", "10000000", "--minc", "10000",
                           "--max-prime", "100", "--min-merit", "5", "--sl", "7500", "--ranges", "1", "-q", *extra],

@@ -45,8 +45,8 @@ def test_sieve_per_x_equals_per_m(oracle):
         assert np.array_equal(rows_x, j.sieve_m(ms))
 
 
-def test_gaps_cfg1_golden(oracle):
-    g = golden("gaps_cfg1.json")
+def test_gaps_P337_golden(oracle):
+    g = golden("gaps_P337_d2310.json")
     ms = np.array(g["ms"], dtype=np.uint64)
     assert len(ms) == 2079
     with oracle.Job(g["P"], g["d"], g["sl"], 1_000_000) as j:
@@ -61,9 +61,9 @@ def test_gaps_cfg1_golden(oracle):
         assert tests > 0
 
 
-def test_records_cfg1(oracle):
+def test_records_P337(oracle):
     import math
-    g = golden("gaps_cfg1.json")
+    g = golden("gaps_P337_d2310.json")
     recs = []
     for m, a, b in zip(g["ms"], g["prev_gap"], g["next_gap"]):
         mer = (a + b) / (g["k_log"] + math.log(m))
@@ -72,7 +72,7 @@ def test_records_cfg1(oracle):
     assert recs == g["records"] and len(recs) > 0
 
 
-@pytest.mark.parametrize("name", ["gaps_cfg2.json", "gaps_cfg3.json"])
+@pytest.mark.parametrize("name", ["gaps_P503_d2190.json", "gaps_P907_d210.json"])
 def test_gaps_samples_golden(oracle, name):
     g = golden(name)
     ms = np.array(g["ms"][:4], dtype=np.uint64)

@@ -15,9 +15,9 @@ def _job(pg, g, **kw):
 
 
 @pytest.mark.parametrize("form", [0, 1])
-def test_cfg1_full_window(pg, form):
+def test_P337_full_window(pg, form):
     """P=337, d=2310, m in [1e7, 1e7+1e4), SL 7500, primes <= 1e8: every gap equals GMP's."""
-    g = golden("gaps_cfg1.json")
+    g = golden("gaps_P337_d2310.json")
     with _job(pg, g) as job:
         assert job.k_log == g["k_log"]
         res = job.search(g["m_start"], g["m_inc"], form)
@@ -31,7 +31,7 @@ def test_cfg1_full_window(pg, form):
             assert st["passes"] > 10
 
 
-@pytest.mark.parametrize("name", ["gaps_cfg2.json", "gaps_cfg3.json"])
+@pytest.mark.parametrize("name", ["gaps_P503_d2190.json", "gaps_P907_d210.json"])
 def test_config_windows_against_gmp(pg, name):
     """The whole P=503 (primes <= 2e9) / P=907 (primes <= 1e10) windows; the GMP-sampled m must match."""
     g = golden(name)
@@ -45,8 +45,8 @@ def test_config_windows_against_gmp(pg, name):
     assert (res.prev_gap % 2 == 0).all() and (res.next_gap % 2 == 0).all()
 
 
-def test_cfg2_sieve_matches_oracle_on_a_sample(pg, oracle):
-    g = golden("gaps_cfg2.json")
+def test_P503_sieve_matches_oracle_on_a_sample(pg, oracle):
+    g = golden("gaps_P503_d2190.json")
     with _job(pg, g) as job:
         ms, rows = job.sieve_interval(g["m_start"], 400)
     with oracle.Job(g["P"], g["d"], g["sl"], g["max_prime"]) as oj:
@@ -150,9 +150,9 @@ def test_group_layout_search_equals_single_thread(pg, tpi):
             assert got.stats["confirm_tests"] == want.stats["confirm_tests"]
 
 
-def test_cfg5_P3001_against_gmp(pg):
+def test_P3001_against_gmp(pg):
     """P=3001, d=2190, X in [-40000, 40000], primes <= 1e10: 4 248-bit operands on 136-word lane groups."""
-    g = golden("gaps_cfg5.json")
+    g = golden("gaps_P3001_d2190.json")
     with pg.Job(g["P"], g["d"], g["sl"], g["max_prime"], max_m_inc=64, max_m=g["m_start"] + g["m_inc"]) as job:
         assert job.info["limbs"] == 136 and job.info["tpi"] == 8
         for m, a, b in zip(g["ms"], g["prev_gap"], g["next_gap"]):
