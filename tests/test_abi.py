@@ -39,7 +39,7 @@ def test_count_m_matches_oracle(pg, oracle, m_start, m_inc, d):
 
 
 def test_counts_of_the_benchmark_windows(pg):
-    # survey figures for the configurations: 2,079 / 52,604 / 11,429 / 26,300 m
+    # coprime m of the four benchmark windows: 2,079 / 52,604 / 11,429 / 26,300
     assert pg.count_m(10_000_000, 10_000, 2310) == 2079
     assert pg.count_m(1_000_000, 200_000, 2190) == 52604
     assert pg.count_m(1_000_000, 50_000, 210) == 11429
