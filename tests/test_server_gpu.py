@@ -24,6 +24,8 @@ MIX = [
     (907, 210, 7_000, 5_000_000, 77_777_777, 900, 3),
     (337, 2310, 60, 1_000_000, 10_000_000, 600, 1),       # sl far below the gaps: continuation
     (503, 2190, 4_000, 5_000_000, 3, 5_000, 1),           # m from 3
+    (3001, 2190, 4_000, 5_000_000, 1_001, 300, 1),        # 136-word operands on lane groups
+    (3001, 2190, 3_000, 5_000_000, 77_001, 200, 2),
 ]
 
 
@@ -47,7 +49,7 @@ def test_mixed_requests_equal_alone(pg):
     assert st["requests_done"] == len(MIX)
     assert st["m_done"] == sum(len(w.ms) for w in want)
     assert st["windows"] > st["launches"]          # launches carried several windows
-    assert st["tables_built"] == 5                 # one set per (p, d, max_prime)
+    assert st["tables_built"] == 6                 # one set per (p, d, max_prime)
 
 
 def test_requests_from_threads_and_next_done(pg):
