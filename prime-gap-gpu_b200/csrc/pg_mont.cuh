@@ -196,7 +196,8 @@ __device__ __forceinline__ void mont_sqr(uint32_t (&x)[L], const uint32_t (&n)[L
     for (int k = 0; k < 2 * L + 2; k++) E[k] = F[k] = 0;
     // cross products x_i * x_j (j > i) at position i + j, row i in two chains
     // (j - i odd, j - i even).  Each array stays below B^(i+L+1) after row i,
-    // so a chain's carry out stops in the word above its top pair.
+    // so a chain's carry out stops in the word above its top pair, and the
+    // chain that ends at j = L - 1 (top pair at i+L-1, i+L) has none at all.
 #pragma unroll
     for (int i = 0; i < L - 1; i++) {
         const uint32_t a = x[i];
@@ -204,25 +205,23 @@ __device__ __forceinline__ void mont_sqr(uint32_t (&x)[L], const uint32_t (&n)[L
         for (int c = 0; c < 2; c++) {
             const int j0 = i + 1 + c;
             if (j0 >= L) continue;
-            int jl = j0;
-#pragma unroll
-            for (int j = j0; j < L; j += 2) jl = j;
+            const int jl = j0 + ((L - 1 - j0) / 2) * 2;
+            const bool top = jl == L - 1;
 #pragma unroll
             for (int j = j0; j < L; j += 2) {
                 const int p = i + j;
-                if ((p & 1) == 0) {
-                    if (j == j0) mad_link<true>(E[p], E[p + 1], a, x[j]);
-                    else mad_link<false>(E[p], E[p + 1], a, x[j]);
-                } else {
-                    if (j == j0) mad_link<true>(F[p - 1], F[p], a, x[j]);
-                    else mad_link<false>(F[p - 1], F[p], a, x[j]);
-                }
+                uint32_t &lo = (p & 1) == 0 ? E[p] : F[p - 1];
+                uint32_t &hi = (p & 1) == 0 ? E[p + 1] : F[p];
+                lo = j == j0 ? mad_lo_cc(a, x[j], lo) : madc_lo_cc(a, x[j], lo);
+                hi = (j == jl && top) ? madc_hi(a, x[j], hi) : madc_hi_cc(a, x[j], hi);
             }
-            const int cp = i + jl + 2;
-            if ((cp & 1) == 0)
-                E[cp] = addc(E[cp], 0u);
-            else
-                F[cp - 1] = addc(F[cp - 1], 0u);
+            if (!top) {
+                const int cp = i + jl + 2;
+                if ((cp & 1) == 0)
+                    E[cp] = addc(E[cp], 0u);
+                else
+                    F[cp - 1] = addc(F[cp - 1], 0u);
+            }
         }
     }
     // double both arrays (each holds less than half of B^(2L))
