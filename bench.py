@@ -283,6 +283,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
     tr = traffic_per_launch()
     roof = {"bound": "imad", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "G limb-products/s",
             "frac": achieved / peak, "traffic": tr.get("bytes_per_launch") if tr else None,
+            "imad_pipe_busy_ncu": tr.get("imad_pipe_busy") if tr else None,
             "kernel": "k_search_persistent<22>",
             "work": f"{ppt} limb products per {bits}-bit test (2*L^2*(B+ceil(B/5)), L=ceil(B/32)), "
                     f"{tests // args.steps} tests per launch",
