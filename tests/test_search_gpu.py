@@ -150,6 +150,20 @@ def test_group_layout_search_equals_single_thread(pg, tpi):
             assert got.stats["confirm_tests"] == want.stats["confirm_tests"]
 
 
+@pytest.mark.parametrize("tpi", [4, 8])
+def test_group_layout_continuation_past_sl(pg, oracle, tpi):
+    """SL far below the gaps on the lane-group kernels: the continuation launches and the trial division
+    of extension positions give GMP's gaps."""
+    m_start, m_inc = 1_000_000, 400
+    with pg.Job(503, 2190, 60, 2_000_000, max_m_inc=m_inc, max_m=m_start + m_inc, tpi=tpi) as job:
+        assert job.info["tpi"] == tpi
+        res = job.search(m_start, m_inc)
+    with oracle.Job(503, 2190, 60, 2_000_000) as oj:
+        prev, nxt = oj.gmp_gaps(res.ms)
+    assert np.array_equal(res.prev_gap, prev) and np.array_equal(res.next_gap, nxt)
+    assert res.stats["extended_sides"] > 0
+
+
 def test_P3001_against_gmp(pg):
     """P=3001, d=2190, X in [-40000, 40000], primes <= 1e10: 4 248-bit operands on 136-word lane groups."""
     g = golden("gaps_P3001_d2190.json")
