@@ -12,6 +12,8 @@
 //   --form persistent|plain   --rounds R   --device N
 //   --warps-per-sm W   cap on each window's PRP warps per SM (default 6; 0 = all that fit):
 //                      two windows are in flight and share the SMs
+//   --resume FILE      after every finished range write "P D MINC NEXT_MSTART RANGES_DONE" to FILE;
+//                      when FILE exists at start (same P, D, MINC), continue from it
 // Record lines "{gap} {merit:.3f} {m} * {P}# / {D} - {prev}" go to stdout and
 // are appended to records_{P}.txt.  Ctrl-C once: finish the current window;
 // twice: stop after the current device call; three times: exit(2)
@@ -50,6 +52,7 @@ struct Config {
     uint32_t rounds = 1;
     int device = 0;
     uint32_t warps_per_sm = 6;
+    std::string resume;
 };
 
 static void show_usage(const char *name) {
@@ -63,7 +66,8 @@ static void show_usage(const char *name) {
     printf("  --chunk <C>     m per device call (default min(minc, 1000000))\n");
     printf("  --form persistent|plain   --rounds <bases>   --device <n>\n");
     printf("  --warps-per-sm <W>  PRP warps per SM of each of the two windows in flight\n");
-    printf("                      (default 6, 0 = as many as fit)\n\n");
+    printf("                      (default 6, 0 = as many as fit)\n");
+    printf("  --resume <file>     progress file: written after every finished range, read at start\n\n");
     printf("[OPTIONAL]\n  -q, --quiet\n  -v, --verbose\n  -h, --help\n");
 }
 
@@ -84,7 +88,7 @@ static Config argparse(int argc, char **argv) {
         {"sl", required_argument, 0, 20},         {"ranges", required_argument, 0, 21},
         {"chunk", required_argument, 0, 22},      {"form", required_argument, 0, 23},
         {"rounds", required_argument, 0, 24},     {"device", required_argument, 0, 25},
-        {"warps-per-sm", required_argument, 0, 26},
+        {"warps-per-sm", required_argument, 0, 26}, {"resume", required_argument, 0, 27},
         {"quiet", no_argument, 0, 'q'},           {"verbose", no_argument, 0, 'v'},
         {"help", no_argument, 0, 'h'},            {0, 0, 0, 0}};
     Config c;
@@ -115,6 +119,7 @@ static Config argparse(int argc, char **argv) {
             case 24: c.rounds = (uint32_t)atoi(optarg); break;
             case 25: c.device = atoi(optarg); break;
             case 26: c.warps_per_sm = (uint32_t)atoi(optarg); break;
+            case 27: c.resume = optarg; break;
             default: c.valid = 0;
         }
     }
@@ -161,8 +166,28 @@ int main(int argc, char **argv) {
         return 1;
     }
     if (c.verbose >= 0) printf("\nTesting m * %u#/%u\n", c.p, c.d);
+    // progress file: continue after the last finished range of the same search
+    uint64_t ranges_done = 0;
+    if (!c.resume.empty()) {
+        if (FILE *f = fopen(c.resume.c_str(), "r")) {
+            unsigned long long fp = 0, fd = 0, finc = 0, fnext = 0, fdone = 0;
+            const int got = fscanf(f, "%llu %llu %llu %llu %llu", &fp, &fd, &finc, &fnext, &fdone);
+            fclose(f);
+            if (got != 5 || fp != c.p || fd != c.d || finc != c.m_inc) {
+                fprintf(stderr, "ERROR %s does not hold the progress of -p %u -d %u --minc %llu\n", c.resume.c_str(),
+                        c.p, c.d, (unsigned long long)c.m_inc);
+                return 1;
+            }
+            c.m_start = fnext;
+            ranges_done = fdone;
+            if (c.verbose >= 0)
+                printf("resuming at m = %llu after %llu ranges\n", (unsigned long long)fnext, (unsigned long long)fdone);
+        }
+    }
+    if (c.ranges && ranges_done >= c.ranges) return 0;
     const uint64_t chunk = c.chunk ? c.chunk : std::min<uint64_t>(c.m_inc, 1000000);
-    const uint64_t last_m = c.ranges ? c.m_start + c.ranges * c.m_inc : c.m_start + 1000 * c.m_inc;
+    const uint64_t last_m =
+        c.ranges ? c.m_start + (c.ranges - ranges_done) * c.m_inc : c.m_start + 1000 * c.m_inc;
     pg_ctx *ctx = nullptr;
     CHECK(pg_ctx_create(c.device, &ctx));
     // default radius: 8 * ln(N), even (the serving configuration's SL)
@@ -248,8 +273,13 @@ int main(int argc, char **argv) {
     };
     uint64_t m_start = c.m_start;
     int next_buf = 0;
-    for (uint64_t r = 0; (c.ranges == 0 || r < c.ranges) && g_stop == 0; r++) {
-        for (uint64_t off = 0; off < c.m_inc && g_stop < 2; off += chunk) {
+    for (uint64_t r = ranges_done; (c.ranges == 0 || r < c.ranges) && g_stop == 0; r++) {
+        bool whole = true;
+        for (uint64_t off = 0; off < c.m_inc; off += chunk) {
+            if (g_stop >= 2) {
+                whole = false;
+                break;
+            }
             const uint64_t inc = std::min(chunk, c.m_inc - off);
             if ((int)pending.size() == PG_SEARCH_SLOTS && finish_one()) return 1;
             uint64_t ticket = 0;
@@ -261,6 +291,15 @@ int main(int argc, char **argv) {
         while (!pending.empty())
             if (finish_one()) return 1;
         m_start += c.m_inc;
+        if (whole && !c.resume.empty()) {  // the range is done: record where the next one starts
+            const std::string tmp = c.resume + ".tmp";
+            if (FILE *f = fopen(tmp.c_str(), "w")) {
+                fprintf(f, "%u %u %llu %llu %llu\n", c.p, c.d, (unsigned long long)c.m_inc,
+                        (unsigned long long)m_start, (unsigned long long)(r + 1));
+                fclose(f);
+                std::rename(tmp.c_str(), c.resume.c_str());
+            }
+        }
         if (c.verbose >= 1) {
             const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
             printf("\nGPU Timings (%.0f seconds):\n", c.show_timing ? secs : 0.0);

@@ -60,3 +60,34 @@ def test_cli_records(pg, tmp_path, extra):
     lines = [line for line in out.splitlines() if rec.match(line)]
     assert lines == g["records"]
     assert (tmp_path / "records_337.txt").read_text().splitlines() == g["records"]
+
+
+def test_cli_resume_file_checks(pg, tmp_path):
+    """A progress file of another search is refused; a finished one ends the run at once (no device use)."""
+    cli = pg.LIB_PATH.parent / "gap_search_gpu"
+    prog = tmp_path / "progress.txt"
+    prog.write_text("337 2310 5000 10005000 1\n")
+    r = subprocess.run([str(cli), "-p", "337", "-d", "210", "--mstart", "10000000", "--minc", "5000",
+                        "--max-prime", "100", "--ranges", "2", "--resume", str(prog), "-q"],
+                       capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 1 and "does not hold the progress" in r.stderr
+    r = subprocess.run([str(cli), "-p", "337", "-d", "2310", "--mstart", "10000000", "--minc", "5000",
+                        "--max-prime", "100", "--ranges", "1", "--resume", str(prog), "-q"],
+                       capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 0 and prog.read_text() == "337 2310 5000 10005000 1\n"
+
+
+@pytest.mark.gpu
+def test_cli_resume_continues(pg, tmp_path):
+    """Two runs with a progress file search the P=337 window's two halves and print its GMP records."""
+    from conftest import golden
+    g = golden("gaps_P337_d2310.json")
+    cli = pg.LIB_PATH.parent / "gap_search_gpu"
+    prog = tmp_path / "progress.txt"
+    base = [str(cli), "-p", "337", "-d", "2310", "--mstart", "10000000", "--minc", "5000", "--max-prime", "100",
+            "--min-merit", "5", "--sl", "7500", "--resume", str(prog), "-q"]
+    subprocess.run(base + ["--ranges", "1"], capture_output=True, text=True, cwd=tmp_path, check=True)
+    assert prog.read_text() == "337 2310 5000 10005000 1\n"
+    subprocess.run(base + ["--ranges", "2"], capture_output=True, text=True, cwd=tmp_path, check=True)
+    assert prog.read_text() == "337 2310 5000 10010000 2\n"
+    assert (tmp_path / "records_337.txt").read_text().splitlines() == g["records"]
