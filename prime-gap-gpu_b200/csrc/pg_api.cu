@@ -516,15 +516,6 @@ bool pg::slot_fits(const Slot &s, const pg_job *j, uint64_t nm, uint64_t nodd) {
     return 2 * (s.nm + nm) * stride <= s.list_cap;
 }
 
-uint32_t pg::count_coprime(uint64_t m_start, uint64_t m_inc, uint32_t d, uint64_t *nodd) {
-    const uint64_t m0 = m_start | 1ull, end = m_start + m_inc;
-    const uint64_t n = end > m0 ? (end - m0 + 1) / 2 : 0;
-    uint64_t c = 0;
-    for (uint64_t i = 0; i < n; i++) c += gcd64(m0 + 2 * i, d) == 1;
-    if (nodd) *nodd = n;
-    return (uint32_t)c;
-}
-
 int pg::slot_add(Slot &s, pg_job *j, uint64_t m_start, uint64_t m_inc) {
     const pg_job_params &p = j->prm;
     if (m_inc == 0) return fail(PG_ERR_ARG, "m_inc must be > 0");

@@ -137,7 +137,6 @@ int slot_enqueue(Slot &s, int form, uint32_t flags, bool graph);
 int slot_finish(Slot &s);
 
 int job_create(pg_ctx *c, const pg_job_params &p, pg_job **out);
-uint32_t count_coprime(uint64_t m_start, uint64_t m_inc, uint32_t d, uint64_t *nodd);
 
 }  // namespace pg
 
