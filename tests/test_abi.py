@@ -84,3 +84,25 @@ def test_server_without_gpu_reports_an_error(pg):
     i = ctypes.c_uint64(0)
     assert pg.lib.pg_server_submit(None, ctypes.byref(rq), ctypes.byref(i)) == -1
     assert pg.lib.pg_server_destroy(None) == 0
+
+
+def test_records_keep_strictly_greater_merits(pg):
+    """records(): merit > min_merit strictly (overflow.cpp:164), exact formula after the numpy pre-filter."""
+    import numpy as np
+    k_log = 303.87395620173214
+    ms = np.array([10_000_003, 10_000_019, 10_000_031], dtype=np.uint64)
+    prev = np.array([300, 1000, 20], dtype=np.uint32)
+    nxt = np.array([392, 1200, 10], dtype=np.uint32)
+    res = pg.SearchResult(ms, prev, nxt, {})
+    m1 = pg.merit(k_log, 10_000_003, 692)
+    assert pg.records(res, k_log, 337, 2310, m1) == [pg.format_record(2200, pg.merit(k_log, 10_000_019, 2200),
+                                                                      10_000_019, 337, 2310, 1000)]
+    assert len(pg.records(res, k_log, 337, 2310, m1 - 1e-9)) == 2
+    assert pg.records(res, k_log, 337, 2310, 100.0) == []
+
+
+def test_format_record_rejects_a_short_buffer(pg):
+    import ctypes
+    buf = ctypes.create_string_buffer(8)
+    rc = pg.lib.pg_format_record(buf, 8, 15234, 22.5, 1000003, 503, 2190, 7342)
+    assert rc == -1 and "too small" in pg.lib.pg_last_error().decode()
