@@ -127,3 +127,18 @@ def test_destroy_fails_queued_requests(pg):
     for k in range(6):
         srv.submit(503, 2190, 3_000, 20_000_000, 1_000_000 + 10_000 * k, 5_000)
     srv.close()  # finishes the launches in flight, fails the rest, frees everything
+
+
+def test_request_larger_than_the_budget_fails(pg):
+    kw = dict(batch_m=2_000, window_m=2_000, max_windows=4, max_sl=4_000)
+    with pg.Server(**kw) as probe:
+        slot_bytes = probe.stats()["resident_bytes"]
+    budget = slot_bytes + int(1.5 * _tables_estimate(5_000_000))
+    with pg.Server(hbm_budget=budget, **kw) as srv:
+        small = srv.submit(337, 2310, 2_000, 5_000_000, 10_000_000, 500)
+        huge = srv.submit(503, 2190, 2_000, 400_000_000, 1_000_000, 500)   # ~240 MB of tables
+        assert len(srv.wait(small).ms) == pg.count_m(10_000_000, 500, 2310)
+        with pytest.raises(pg.PrimeGapError) as e:
+            srv.wait(huge, timeout=120.0)
+        assert e.value.code == -4 and "exceed the budget" in str(e.value)
+        assert srv.stats()["peak_bytes"] <= budget
