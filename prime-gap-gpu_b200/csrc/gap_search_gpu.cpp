@@ -14,6 +14,8 @@
 //                      two windows are in flight and share the SMs
 //   --resume FILE      after every finished range write "P D MINC NEXT_MSTART RANGES_DONE" to FILE;
 //                      when FILE exists at start (same P, D, MINC), continue from it
+//   --devices A,B,...  one worker per listed CUDA device, each searching whole ranges (the m ranges
+//                      shard with no exchange); records are printed in range order
 // Record lines "{gap} {merit:.3f} {m} * {P}# / {D} - {prev}" go to stdout and
 // are appended to records_{P}.txt.  Ctrl-C once: finish the current window;
 // twice: stop after the current device call; three times: exit(2)
@@ -27,8 +29,12 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <condition_variable>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/primegap.h"
@@ -53,6 +59,7 @@ struct Config {
     int device = 0;
     uint32_t warps_per_sm = 6;
     std::string resume;
+    std::vector<int> devices;  // --devices; empty = {device}
 };
 
 static void show_usage(const char *name) {
@@ -67,7 +74,8 @@ static void show_usage(const char *name) {
     printf("  --form persistent|plain   --rounds <bases>   --device <n>\n");
     printf("  --warps-per-sm <W>  PRP warps per SM of each of the two windows in flight\n");
     printf("                      (default 6, 0 = as many as fit)\n");
-    printf("  --resume <file>     progress file: written after every finished range, read at start\n\n");
+    printf("  --resume <file>     progress file: written after every finished range, read at start\n");
+    printf("  --devices <a,b,..>  search on these CUDA devices, one range per device at a time\n\n");
     printf("[OPTIONAL]\n  -q, --quiet\n  -v, --verbose\n  -h, --help\n");
 }
 
@@ -89,6 +97,7 @@ static Config argparse(int argc, char **argv) {
         {"chunk", required_argument, 0, 22},      {"form", required_argument, 0, 23},
         {"rounds", required_argument, 0, 24},     {"device", required_argument, 0, 25},
         {"warps-per-sm", required_argument, 0, 26}, {"resume", required_argument, 0, 27},
+        {"devices", required_argument, 0, 28},
         {"quiet", no_argument, 0, 'q'},           {"verbose", no_argument, 0, 'v'},
         {"help", no_argument, 0, 'h'},            {0, 0, 0, 0}};
     Config c;
@@ -120,6 +129,18 @@ static Config argparse(int argc, char **argv) {
             case 25: c.device = atoi(optarg); break;
             case 26: c.warps_per_sm = (uint32_t)atoi(optarg); break;
             case 27: c.resume = optarg; break;
+            case 28:
+                for (const char *q = optarg; *q;) {
+                    char *end = nullptr;
+                    const long v = strtol(q, &end, 10);
+                    if (end == q || v < 0 || (*end && *end != ',')) {
+                        c.valid = 0;
+                        break;
+                    }
+                    c.devices.push_back((int)v);
+                    q = *end == ',' ? end + 1 : end;
+                }
+                break;
             default: c.valid = 0;
         }
     }
@@ -159,6 +180,90 @@ static void on_sigint(int) {
         }                                                                        \
     } while (0)
 
+// One device's context and job, with the host buffers of its PG_SEARCH_SLOTS
+// windows in flight.
+struct Engine {
+    Engine() = default;
+    Engine(const Engine &) = delete;
+    Engine &operator=(const Engine &) = delete;
+    pg_ctx *ctx = nullptr;
+    pg_job *job = nullptr;
+    pg_job_info info{};
+    std::vector<uint64_t> ms[PG_SEARCH_SLOTS];
+    std::vector<uint32_t> prev[PG_SEARCH_SLOTS], next[PG_SEARCH_SLOTS];
+    ~Engine() {
+        if (job) pg_job_destroy(job);
+        if (ctx) pg_ctx_destroy(ctx);
+    }
+};
+
+// The records and counts of one range of --minc m.
+struct RangeOut {
+    std::vector<std::string> lines;
+    uint64_t m = 0, tests = 0, ext = 0;
+    bool whole = true;  // false when a second Ctrl-C stopped it part-way
+    bool done = false;
+};
+
+static int make_engine(Engine &e, int device, const pg_job_params &prm, uint64_t chunk) {
+    CHECK(pg_ctx_create(device, &e.ctx));
+    CHECK(pg_job_create(e.ctx, &prm, &e.job));
+    pg_job_get_info(e.job, &e.info);
+    for (int k = 0; k < PG_SEARCH_SLOTS; k++) {
+        e.ms[k].resize(chunk);
+        e.prev[k].resize(chunk);
+        e.next[k].resize(chunk);
+    }
+    return 0;
+}
+
+// Searches [m_start, m_start + m_inc) in chunks with PG_SEARCH_SLOTS windows in
+// flight: while one window's gaps are read, the next runs on the device.
+static int search_range(Engine &e, const Config &c, uint64_t chunk, uint64_t m_start, RangeOut &out) {
+    struct Pending {
+        uint64_t ticket;
+        int buf;
+    };
+    const uint32_t flags = c.form == PG_SEARCH_PERSISTENT ? PG_SUBMIT_WARPS_PER_SM(c.warps_per_sm) : 0u;
+    std::vector<Pending> pending;
+    auto finish_one = [&]() {
+        const Pending pd = pending.front();
+        pending.erase(pending.begin());
+        pg_search_stats st{};
+        CHECK(pg_search_wait(e.job, pd.ticket, e.ms[pd.buf].data(), e.prev[pd.buf].data(), e.next[pd.buf].data(),
+                             &st));
+        out.m += st.m_count;
+        out.tests += st.prp_tests;
+        out.ext += st.extended_sides;
+        for (uint64_t i = 0; i < st.m_count; i++) {
+            const uint64_t gap = (uint64_t)e.prev[pd.buf][i] + e.next[pd.buf][i];
+            const double merit = pg_merit(e.info.k_log, e.ms[pd.buf][i], gap);
+            if (merit > c.min_merit) {
+                char line[160];
+                pg_format_record(line, sizeof line, gap, merit, e.ms[pd.buf][i], c.p, c.d, e.prev[pd.buf][i]);
+                out.lines.push_back(line);
+            }
+        }
+        return 0;
+    };
+    int next_buf = 0;
+    for (uint64_t off = 0; off < c.m_inc; off += chunk) {
+        if (g_stop >= 2) {
+            out.whole = false;
+            break;
+        }
+        const uint64_t inc = std::min(chunk, c.m_inc - off);
+        if ((int)pending.size() == PG_SEARCH_SLOTS && finish_one()) return 1;
+        uint64_t ticket = 0;
+        CHECK(pg_search_submit(e.job, m_start + off, inc, c.form, flags, &ticket));
+        pending.push_back({ticket, next_buf});
+        next_buf = (next_buf + 1) % PG_SEARCH_SLOTS;
+    }
+    while (!pending.empty())
+        if (finish_one()) return 1;
+    return 0;
+}
+
 int main(int argc, char **argv) {
     Config c = argparse(argc, argv);
     if (!c.valid) {
@@ -188,8 +293,7 @@ int main(int argc, char **argv) {
     const uint64_t chunk = c.chunk ? c.chunk : std::min<uint64_t>(c.m_inc, 1000000);
     const uint64_t last_m =
         c.ranges ? c.m_start + (c.ranges - ranges_done) * c.m_inc : c.m_start + 1000 * c.m_inc;
-    pg_ctx *ctx = nullptr;
-    CHECK(pg_ctx_create(c.device, &ctx));
+    if (c.devices.empty()) c.devices.push_back(c.device);
     // default radius: 8 * ln(N), even (the serving configuration's SL)
     uint32_t sl = c.sl;
     pg_job_params prm{};
@@ -201,27 +305,32 @@ int main(int argc, char **argv) {
     prm.rounds = c.rounds;
     if (!sl) {
         // log(K) first from a throw-away job with a tiny radius
+        pg_ctx *pctx = nullptr;
+        CHECK(pg_ctx_create(c.devices[0], &pctx));
         pg_job *probe = nullptr;
         pg_job_params pp = prm;
         pp.sl = 2;
         pp.max_prime = std::min<uint64_t>(c.max_prime, 1000);
         pp.max_m_inc = 2;
-        CHECK(pg_job_create(ctx, &pp, &probe));
+        CHECK(pg_job_create(pctx, &pp, &probe));
         pg_job_info pi{};
         pg_job_get_info(probe, &pi);
         pg_job_destroy(probe);
+        pg_ctx_destroy(pctx);
         sl = 2 * (uint32_t)std::lround(4.0 * (pi.k_log + std::log((double)c.m_start)));
     }
     prm.sl = sl;
-    pg_job *job = nullptr;
-    CHECK(pg_job_create(ctx, &prm, &job));
-    pg_job_info info{};
-    pg_job_get_info(job, &info);
+    const size_t ndev = c.devices.size();
+    std::vector<Engine> eng(ndev);
+    for (size_t k = 0; k < ndev; k++)
+        if (make_engine(eng[k], c.devices[k], prm, chunk)) return 1;
+    const pg_job_info &info = eng[0].info;
     if (c.verbose >= 1) {
         printf("K = %u bits, log(K) = %.2f\n", info.k_bits, info.k_log);
         printf("sieve: %llu primes <= %llu, X in [-%u, %u], %u-word operands\n",
                (unsigned long long)info.num_primes + info.num_small, (unsigned long long)c.max_prime, sl, sl,
                info.limbs);
+        if (ndev > 1) printf("devices: %zu, each searching whole ranges of %llu m\n", ndev, (unsigned long long)c.m_inc);
         if (c.show_timing) printf("\tSetup took %.1f seconds\n", info.setup_seconds);
         printf("Min Gap ~= %d (for merit > %.1f)\n", (int)(c.min_merit * (info.k_log + std::log((double)c.m_inc))),
                c.min_merit);
@@ -230,72 +339,61 @@ int main(int argc, char **argv) {
     char fname[64];
     snprintf(fname, sizeof fname, "records_%u.txt", c.p);
     FILE *rec = fopen(fname, "a");
-    // PG_SEARCH_SLOTS windows in flight: while one window's gaps are read and
-    // its records written, the next window runs on the device
-    struct Pending {
-        uint64_t ticket;
-        int buf;
-    };
-    std::vector<uint64_t> ms[PG_SEARCH_SLOTS];
-    std::vector<uint32_t> prev[PG_SEARCH_SLOTS], next[PG_SEARCH_SLOTS];
-    for (int k = 0; k < PG_SEARCH_SLOTS; k++) {
-        ms[k].resize(chunk);
-        prev[k].resize(chunk);
-        next[k].resize(chunk);
-    }
-    const uint32_t flags = c.form == PG_SEARCH_PERSISTENT ? PG_SUBMIT_WARPS_PER_SM(c.warps_per_sm) : 0u;
-    std::vector<Pending> pending;
     uint64_t total_m = 0, total_tests = 0, total_primes = 0, total_ext = 0;
     const auto t0 = std::chrono::steady_clock::now();
-    auto finish_one = [&]() {
-        const Pending pd = pending.front();
-        pending.erase(pending.begin());
-        pg_search_stats st{};
-        CHECK(pg_search_wait(job, pd.ticket, ms[pd.buf].data(), prev[pd.buf].data(), next[pd.buf].data(), &st));
-        total_m += st.m_count;
-        total_tests += st.prp_tests;
-        total_primes += 2 * st.m_count;
-        total_ext += st.extended_sides;
-        for (uint64_t i = 0; i < st.m_count; i++) {
-            const uint64_t gap = (uint64_t)prev[pd.buf][i] + next[pd.buf][i];
-            const double merit = pg_merit(info.k_log, ms[pd.buf][i], gap);
-            if (merit > c.min_merit) {
-                char line[160];
-                pg_format_record(line, sizeof line, gap, merit, ms[pd.buf][i], c.p, c.d, prev[pd.buf][i]);
-                printf("%s\n", line);
-                if (rec) {
-                    fprintf(rec, "%s\n", line);
-                    fflush(rec);
-                }
-            }
-        }
-        return 0;
-    };
-    uint64_t m_start = c.m_start;
-    int next_buf = 0;
-    for (uint64_t r = ranges_done; (c.ranges == 0 || r < c.ranges) && g_stop == 0; r++) {
-        bool whole = true;
-        for (uint64_t off = 0; off < c.m_inc; off += chunk) {
-            if (g_stop >= 2) {
-                whole = false;
+    // Ranges are handed to the devices in order; each range's records are
+    // printed, and the progress file advanced, in range order.
+    std::mutex mu;
+    std::condition_variable cv;
+    std::map<uint64_t, RangeOut> finished;
+    std::atomic<uint64_t> next_range{ranges_done};
+    std::atomic<int> failed{0};
+    std::atomic<size_t> stopped{0};  // workers that have exited
+    auto worker = [&](size_t k) {
+        while (g_stop == 0 && !failed) {
+            const uint64_t r = next_range++;
+            if (c.ranges && r >= c.ranges) break;
+            RangeOut out;
+            if (search_range(eng[k], c, chunk, c.m_start + (r - ranges_done) * c.m_inc, out)) {
+                failed = 1;
                 break;
             }
-            const uint64_t inc = std::min(chunk, c.m_inc - off);
-            if ((int)pending.size() == PG_SEARCH_SLOTS && finish_one()) return 1;
-            uint64_t ticket = 0;
-            CHECK(pg_search_submit(job, m_start + off, inc, c.form, flags, &ticket));
-            pending.push_back({ticket, next_buf});
-            next_buf = (next_buf + 1) % PG_SEARCH_SLOTS;
+            std::lock_guard<std::mutex> lk(mu);
+            finished[r] = std::move(out);
+            cv.notify_all();
         }
-        // the range's last windows finish before its summary
-        while (!pending.empty())
-            if (finish_one()) return 1;
-        m_start += c.m_inc;
-        if (whole && !c.resume.empty()) {  // the range is done: record where the next one starts
+        std::lock_guard<std::mutex> lk(mu);
+        stopped++;
+        cv.notify_all();
+    };
+    std::vector<std::thread> threads;
+    for (size_t k = 0; k < ndev; k++) threads.emplace_back(worker, k);
+    // print the ranges in order as they finish
+    bool contiguous = true;  // every range so far searched whole: the progress file may advance
+    for (uint64_t r = ranges_done;; r++) {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return finished.count(r) || stopped == ndev; });
+        auto it = finished.find(r);
+        if (it == finished.end()) break;  // every worker has stopped and range r never ran
+        RangeOut out = std::move(it->second);
+        finished.erase(it);
+        lk.unlock();
+        for (const auto &line : out.lines) {
+            printf("%s\n", line.c_str());
+            if (rec) fprintf(rec, "%s\n", line.c_str());
+        }
+        if (rec) fflush(rec);
+        total_m += out.m;
+        total_tests += out.tests;
+        total_primes += 2 * out.m;
+        total_ext += out.ext;
+        contiguous = contiguous && out.whole;
+        if (contiguous && !c.resume.empty()) {  // the range is done: record where the next one starts
             const std::string tmp = c.resume + ".tmp";
             if (FILE *f = fopen(tmp.c_str(), "w")) {
                 fprintf(f, "%u %u %llu %llu %llu\n", c.p, c.d, (unsigned long long)c.m_inc,
-                        (unsigned long long)m_start, (unsigned long long)(r + 1));
+                        (unsigned long long)(c.m_start + (r + 1 - ranges_done) * c.m_inc),
+                        (unsigned long long)(r + 1));
                 fclose(f);
                 std::rename(tmp.c_str(), c.resume.c_str());
             }
@@ -309,8 +407,7 @@ int main(int argc, char **argv) {
             printf("\tpast sl         : %llu sides (continued on the device)\n\n", (unsigned long long)total_ext);
         }
     }
+    for (auto &t : threads) t.join();
     if (rec) fclose(rec);
-    pg_job_destroy(job);
-    pg_ctx_destroy(ctx);
-    return 0;
+    return failed ? 1 : 0;
 }

@@ -91,3 +91,28 @@ def test_cli_resume_continues(pg, tmp_path):
     subprocess.run(base + ["--ranges", "2"], capture_output=True, text=True, cwd=tmp_path, check=True)
     assert prog.read_text() == "337 2310 5000 10010000 2\n"
     assert (tmp_path / "records_337.txt").read_text().splitlines() == g["records"]
+
+
+@pytest.mark.gpu
+def test_cli_two_workers_print_ranges_in_order(pg, tmp_path):
+    """--devices 0,0: two workers (two contexts on one device here; one per GPU on a multi-GPU node) take
+    the two halves of the P=337 window; the records come out in m order and equal GMP's."""
+    from conftest import golden
+    g = golden("gaps_P337_d2310.json")
+    cli = pg.LIB_PATH.parent / "gap_search_gpu"
+    prog = tmp_path / "progress.txt"
+    out = subprocess.run([str(cli), "-p", "337", "-d", "2310", "--mstart", "10000000", "--minc", "2500",
+                          "--max-prime", "100", "--min-merit", "5", "--sl", "7500", "--ranges", "4",
+                          "--devices", "0,0", "--resume", str(prog), "-q"],
+                         capture_output=True, text=True, cwd=tmp_path, check=True).stdout
+    import re
+    rec = re.compile(r"^\d+ \d+\.\d{3} \d+ \* \d+# / \d+ - \d+$")
+    assert [line for line in out.splitlines() if rec.match(line)] == g["records"]
+    assert prog.read_text() == "337 2310 2500 10010000 4\n"
+
+
+def test_cli_rejects_a_bad_device_list(pg):
+    cli = pg.LIB_PATH.parent / "gap_search_gpu"
+    r = subprocess.run([str(cli), "-p", "337", "-d", "2310", "--mstart", "1", "--minc", "10", "--max-prime", "1",
+                        "--devices", "0,x"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Usage" in r.stdout
