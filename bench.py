@@ -417,11 +417,16 @@ def run_serve(args) -> dict:
         th.join()
         lat = np.array([(lambda x: x["done_s"] - x["submit_s"])(srv.wait(i).info) for i in ids2]) * 1e3
         st = srv.stats()
+        by_p = {}
+        for P in sorted({r[0] for r in reqs}):
+            sel = np.array([r[0] == P for r in reqs])
+            by_p[str(P)] = {"n": int(sel.sum()), "p50_ms": round(float(np.percentile(lat[sel], 50)), 1),
+                            "p99_ms": round(float(np.percentile(lat[sel], 99)), 1)}
     return {
         "metric": "serving latency p99 (256 gap-search requests, Poisson arrivals at 70% of capacity)",
         "value": round(float(np.percentile(lat, 99)), 2), "unit": "ms", "higher_is_better": False,
         "p50_ms": round(float(np.percentile(lat, 50)), 2), "p99_ms": round(float(np.percentile(lat, 99)), 2),
-        "mean_ms": round(float(lat.mean()), 2),
+        "mean_ms": round(float(lat.mean()), 2), "latency_by_P": by_p,
         "capacity_jobs_per_s": round(cap_jobs, 2), "capacity_m_per_s": round(m_total / span, 1),
         "arrival_rate_jobs_per_s": round(rate, 2), "closed_loop_s": round(span, 3),
         "table_build_s": round(table_s, 3),
