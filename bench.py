@@ -142,7 +142,7 @@ def cpu_reference_estimate(threads: int, rows_per_thread: int = 1, seed: int = 1
     prp_s = len(ms_all) * tests_per_m * per_test / threads
     total = sieve_s + prp_s
     job.close()
-    return {"value": len(ms_all) / total, "unit": "m/s", "cores": threads, "kind": "port",
+    return {"value": len(ms_all) / total, "unit": "m/s", "cores": threads, "kind": "port", "cpu": cpu_model(),
             "sample": (f"{R} of {len(real)} sieve rows (X coprime to K) over all {len(ms_all)} m, "
                        f"scaled; PRP tests/m from the oracle search of {len(sample_ms)} m "
                        f"({tests_per_m:.1f}/m); {len(cands)} GMP strong base-2 tests timed "
@@ -150,6 +150,16 @@ def cpu_reference_estimate(threads: int, rows_per_thread: int = 1, seed: int = 1
             "sieve_seconds_full": sieve_s, "prp_seconds_full": prp_s,
             "prp_tests_per_sec": len(ms_all) * tests_per_m / total,
             "sample_seconds": t_rows + t_search + t_prp, "table_setup_seconds": setup_s}
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def host_threads() -> int:
@@ -336,7 +346,7 @@ def run_reference(args) -> dict:
             "config": {"workload": workload_name(WORKLOAD["m_start"], WORKLOAD["m_inc"]),
                        "implementation": "CPU restatement of the reference path (oracle/, GMP 6.3.0); "
                                          "the reference needs CGBN and primesieve, absent here"},
-            "cpu_baseline": {**{k: last[k] for k in ("unit", "cores", "kind", "sample")}, "value": v},
+            "cpu_baseline": {**{k: last[k] for k in ("unit", "cores", "kind", "sample", "cpu")}, "value": v},
             "e2e": {"value": v, "unit": "m/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "prp_tests_per_sec": last["prp_tests_per_sec"]}
 
