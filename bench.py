@@ -7,9 +7,14 @@ strong base-2 PRP outward from X = 0 for the previous and the next prime,
 records of merit > 22.  A step is one search of that window (sieve + PRP +
 finalize), the inputs being the window bounds; the prime tables (98 M primes,
 1.18 GB with their K mod p and K^-1 residues) are read again by every step, far
-more than the 126 MB L2, so no L2 flush is needed between steps.
+more than the 126 MB L2, so no L2 flush is needed between steps.  Two windows
+are in flight (two slots of the job, each with its own stream), each window's
+PRP kernel holding at most 6 warps per SM, so one window's tail runs beside the
+next window's sieve and search; `value` is the m of the K timed windows over
+the device span from the first to the last of them.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --serve      the serving mix instead: capacity and p50/p99 latency
 
 Under torchrun each rank searches its own window of 200,000 m (weak scaling,
 no data-path collective); the reported time is the max over ranks.
