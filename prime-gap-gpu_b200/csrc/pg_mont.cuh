@@ -1,11 +1,12 @@
 // pg_mont.cuh -- multi-precision Montgomery arithmetic for the strong PRP test.
 //
-// One thread owns one L-word number: the operand, the modulus and the 2L+1
-// word double-width accumulator all live in registers (the loops below are
-// fully unrolled over the compile-time L, so every array index is a
-// constant).  Products use PTX multiply-add carry chains (mad.lo.cc /
-// madc.hi.cc), i.e. integer multiply-add only -- no floating point and no
-// tensor cores: this is exact multi-precision integer arithmetic.
+// One thread owns one L-word number: the operand, the modulus and the
+// double-width accumulator (two arrays, see "Register layout" below) all live
+// in registers (the loops below are fully unrolled over the compile-time L,
+// so every array index is a constant).  Products use PTX multiply-add carry
+// chains (mad.lo.cc / madc.hi.cc, fused by ptxas into one 64-bit multiply-add
+// per limb product), i.e. integer multiply-add only -- no floating point and
+// no tensor cores: this is exact multi-precision integer arithmetic.
 //
 // The reference computes the same test with CGBN (miller_rabin.h:160-248):
 // a fixed-window Montgomery powm followed by a squaring chain.  Here the
