@@ -207,3 +207,49 @@ def test_repeat_is_deterministic(pg):
         a = job.search(10_000_000, 3_000)
         b = job.search(10_000_000, 3_000)
     assert np.array_equal(a.prev_gap, b.prev_gap) and np.array_equal(a.next_gap, b.next_gap)
+
+
+def _random_shapes(n: int, seed: int = 2026):
+    """Seeded search shapes: P a prime in [11, 700], d an even divisor of P# made of small primes, sl, the
+    sieve limit, an m range of 1-300 m starting anywhere below 1e12, the form and threads per number."""
+    import random
+    rng = random.Random(seed)
+    primes = [q for q in range(11, 700) if all(q % r for r in range(2, int(q ** 0.5) + 1))]
+    out = []
+    while len(out) < n:
+        P = rng.choice(primes)
+        small = [q for q in (3, 5, 7, 11, 13) if q <= P]
+        d = 2
+        for q in small:
+            if rng.random() < 0.5:
+                d *= q
+        sl = rng.choice([2, 30, 400, 2_000, 9_000])
+        limit = rng.choice([10_000, 200_000, 3_000_000])
+        m_inc = rng.randint(1, 300)
+        m_start = rng.choice([1, rng.randint(1, 10**6), rng.randint(1, 10**12)])
+        out.append((P, d, sl, limit, m_start, m_inc, rng.choice([0, 1]), rng.choice([0, 1, 4])))
+    return out
+
+
+@pytest.mark.parametrize("shape", _random_shapes(24))
+def test_random_shapes_against_gmp(pg, oracle, shape):
+    """Every gap of a seeded random search shape equals GMP's (prevprime / nextprime of m*K)."""
+    P, d, sl, limit, m_start, m_inc, form, tpi = shape
+    K = 1
+    for q in range(2, P + 1):
+        if all(q % r for r in range(2, int(q ** 0.5) + 1)):
+            K *= q
+    K //= d
+    if K <= limit + 2 * sl + 2:
+        pytest.skip("K below the sieve limit")
+    try:
+        job = pg.Job(P, d, sl, limit, max_m_inc=m_inc, max_m=m_start + m_inc, tpi=tpi)
+    except pg.PrimeGapError as e:
+        assert e.code == -3  # no compiled layout of that width for the requested tpi
+        return
+    with job:
+        res = job.search(m_start, m_inc, form)
+    assert len(res.ms) == pg.count_m(m_start, m_inc, d)
+    with oracle.Job(P, d, sl, limit) as oj:
+        prev, nxt = oj.gmp_gaps(res.ms)
+    assert np.array_equal(res.prev_gap, prev) and np.array_equal(res.next_gap, nxt)
