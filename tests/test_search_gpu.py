@@ -211,7 +211,8 @@ def test_repeat_is_deterministic(pg):
 
 def _random_shapes(n: int, seed: int = 2026):
     """Seeded search shapes: P a prime in [11, 700], d an even divisor of P# made of small primes, sl, the
-    sieve limit, an m range of 1-300 m starting anywhere below 1e12, the form and threads per number."""
+    sieve limit, an m range of 1-300 m starting anywhere below 1e12, the form, threads per number and
+    confirmation rounds."""
     import random
     rng = random.Random(seed)
     primes = [q for q in range(11, 700) if all(q % r for r in range(2, int(q ** 0.5) + 1))]
@@ -227,14 +228,14 @@ def _random_shapes(n: int, seed: int = 2026):
         limit = rng.choice([10_000, 200_000, 3_000_000])
         m_inc = rng.randint(1, 300)
         m_start = rng.choice([1, rng.randint(1, 10**6), rng.randint(1, 10**12)])
-        out.append((P, d, sl, limit, m_start, m_inc, rng.choice([0, 1]), rng.choice([0, 1, 4])))
+        out.append((P, d, sl, limit, m_start, m_inc, rng.choice([0, 1]), rng.choice([0, 1, 4]), rng.choice([1, 1, 2])))
     return out
 
 
-@pytest.mark.parametrize("shape", _random_shapes(24))
+@pytest.mark.parametrize("shape", _random_shapes(48))
 def test_random_shapes_against_gmp(pg, oracle, shape):
     """Every gap of a seeded random search shape equals GMP's (prevprime / nextprime of m*K)."""
-    P, d, sl, limit, m_start, m_inc, form, tpi = shape
+    P, d, sl, limit, m_start, m_inc, form, tpi, rounds = shape
     K = 1
     for q in range(2, P + 1):
         if all(q % r for r in range(2, int(q ** 0.5) + 1)):
@@ -243,7 +244,7 @@ def test_random_shapes_against_gmp(pg, oracle, shape):
     if K <= limit + 2 * sl + 2:
         pytest.skip("K below the sieve limit")
     try:
-        job = pg.Job(P, d, sl, limit, max_m_inc=m_inc, max_m=m_start + m_inc, tpi=tpi)
+        job = pg.Job(P, d, sl, limit, max_m_inc=m_inc, max_m=m_start + m_inc, tpi=tpi, rounds=rounds)
     except pg.PrimeGapError as e:
         assert e.code == -3  # no compiled layout of that width for the requested tpi
         return

@@ -89,3 +89,36 @@ def test_bad_jobs_are_errors(pg, bad):
     kw.update(bad)
     with pytest.raises(pg.PrimeGapError):
         pg.Job(**kw)
+
+
+def _random_sieve_shapes(n: int, seed: int = 77):
+    """Seeded sieve shapes: P, d (even divisor of P# of small primes), sl, limit, small-prime bound, m range."""
+    import random
+    rng = random.Random(seed)
+    primes = [q for q in range(40, 1000) if all(q % r for r in range(2, int(q ** 0.5) + 1))]
+    out = []
+    for _ in range(n):
+        P = rng.choice(primes)
+        d = 2
+        for q in (3, 5, 7, 11, 13, 73):
+            if q <= P and rng.random() < 0.4:
+                d *= q
+        sl = rng.choice([2, 7, 64, 1_000, 5_000, 30_000])
+        limit = rng.choice([5_000, 100_000, 2_000_000, 30_000_000])
+        small = rng.choice([0, 2_000, 20_000, 200_000])
+        m_inc = rng.randint(1, 2_000)
+        m_start = rng.choice([1, rng.randint(1, 10**7), rng.randint(1, 10**13)])
+        out.append((P, d, sl, limit, small, m_start, m_inc))
+    return out
+
+
+@pytest.mark.parametrize("shape", _random_sieve_shapes(20))
+def test_random_sieve_rows(pg, oracle, shape):
+    """Every bit of every row of a seeded random sieve shape equals the oracle's."""
+    P, d, sl, limit, small, m_start, m_inc = shape
+    with _job(pg, P, d, sl, limit, m_start, m_inc, small_limit=small) as job:
+        ms, rows = job.sieve_interval(m_start, m_inc)
+    with oracle.Job(P, d, sl, limit) as oj:
+        assert np.array_equal(ms, oracle.coprime_ms(m_start, m_inc, d))
+        want = oj.sieve_m(ms)
+    assert np.array_equal(rows, want)
