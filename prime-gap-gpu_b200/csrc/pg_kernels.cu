@@ -320,6 +320,33 @@ __global__ void __launch_bounds__(256) k_sieve_large_step(const __grid_constant_
 
 // ------------------------------------------------------ modular search
 
+// x mod A for one divisor A >= 1 and several x.  32-bit operands use the
+// integer remainder.  64-bit operands (x < 2^40) use a double-precision
+// reciprocal: x is exact as a double, 1/A and the product x * (1/A) are each
+// rounded once (relative error 2^-53 each), so the quotient estimate
+// trunc(x * (1/A)) is within one of floor(x / A) (x / A < 2^40, absolute
+// error below 2^-12), and the remainder x - q*A, exact in signed 64-bit
+// arithmetic, needs at most one correction either way.
+template <typename U>
+struct DivBy {
+    U A;
+    __device__ __forceinline__ explicit DivBy(U a) : A(a) {}
+    __device__ __forceinline__ U rem(U x) const { return x % A; }
+};
+template <>
+struct DivBy<uint64_t> {
+    uint64_t A;
+    double inv;
+    __device__ __forceinline__ explicit DivBy(uint64_t a) : A(a), inv(1.0 / (double)a) {}
+    __device__ __forceinline__ uint64_t rem(uint64_t x) const {
+        const uint64_t q = (uint64_t)((double)x * inv);
+        int64_t r = (int64_t)(x - q * A);
+        if (r < 0) r += (int64_t)A;
+        if (r >= (int64_t)A) r -= (int64_t)A;
+        return (uint64_t)r;
+    }
+};
+
 // For 0 < A < M, B < M, W < M - 1 and gcd(A, M) = 1, the value
 // u = (A*x + B) mod M at the smallest x >= 0 with (A*x + B) mod M <= W.
 // If B <= W, x = 0 and u = B.  If W + 1 >= A the first wrap already lands in
@@ -339,13 +366,14 @@ __device__ __forceinline__ U modsearch_value(U A, U B, U M, U W) {
             u = B;
             break;
         }
+        const DivBy<U> by(A);
         if (W + 1 >= A) {
-            const U t = (M - B) % A;
+            const U t = by.rem(M - B);
             u = t ? A - t : 0;
             break;
         }
-        const U r = M % A;
-        U b1 = B % A;
+        const U r = by.rem(M);
+        U b1 = by.rem(B);
         b1 = b1 >= r ? b1 - r : b1 + (A - r);  // (B - M) mod A
         B = W >= b1 ? W - b1 : W + (A - b1);   // reflected
         M = A;
@@ -378,13 +406,27 @@ struct Mod32 {
     __device__ __forceinline__ uint32_t sub(uint32_t a, uint32_t b) const { return a >= b ? a - b : a + (p - b); }
 };
 
-// The same for primes in [2^32, 2^40) (products of 40-bit residues split so
-// every partial product fits 64 bits).
+// The same for primes in [2^32, 2^40).  For v < 2^64 the estimate
+// trunc(v * (1/p)) is within one of floor(v / p) (quotient below 2^32,
+// relative error 3 * 2^-53); for a, b < p the estimate of floor(a*b / p)
+// from the double product a*b (rounded) times 1/p is within one too
+// (quotient below 2^40, absolute error below 2^-11).  The remainder is the
+// low 64 bits of v - q*p (or a*b - q*p), exact as a signed value in
+// (-p, 2p), corrected once either way.
 struct Mod40 {
     uint64_t p;
-    __device__ __forceinline__ explicit Mod40(uint64_t q) : p(q) {}
-    __device__ __forceinline__ uint64_t red(uint64_t v) const { return v % p; }
-    __device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) const { return mulmod40(a, b, p); }
+    double inv;
+    __device__ __forceinline__ explicit Mod40(uint64_t q) : p(q), inv(1.0 / (double)q) {}
+    __device__ __forceinline__ uint64_t fix(uint64_t x, uint64_t q) const {
+        int64_t r = (int64_t)(x - q * p);
+        if (r < 0) r += (int64_t)p;
+        if (r >= (int64_t)p) r -= (int64_t)p;
+        return (uint64_t)r;
+    }
+    __device__ __forceinline__ uint64_t red(uint64_t v) const { return fix(v, (uint64_t)((double)v * inv)); }
+    __device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) const {
+        return fix(a * b, (uint64_t)((double)a * (double)b * inv));
+    }
     __device__ __forceinline__ uint64_t sub(uint64_t a, uint64_t b) const { return a >= b ? a - b : a + (p - b); }
 };
 

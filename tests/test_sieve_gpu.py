@@ -56,9 +56,12 @@ def test_large_prime_methods_agree(pg, oracle, flags, P, d, sl, limit, m_start, 
     assert np.array_equal(rows, want)
 
 
-def test_wide_primes_above_2_32(pg, oracle):
+@pytest.mark.parametrize("P,d,sl,limit,m_start,m_inc", [
+    (503, 2190, 4_000, 4_300_000_000, 1_000_000, 60),
+    (211, 2310, 300, 4_400_000_000, 10**12 + 1, 60),    # m above 2^32, short rows
+])
+def test_wide_primes_above_2_32(pg, oracle, P, d, sl, limit, m_start, m_inc):
     """max_prime above 2^32: 64-bit prime tables and residues."""
-    P, d, sl, limit, m_start, m_inc = 503, 2190, 4_000, 4_300_000_000, 1_000_000, 60
     with _job(pg, P, d, sl, limit, m_start, m_inc) as job:
         ms, rows = job.sieve_interval(m_start, m_inc)
         assert job.info["num_primes"] > 200_000_000
