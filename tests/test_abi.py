@@ -5,6 +5,7 @@ from __future__ import annotations
 import math
 import re
 import subprocess
+import sys
 
 import pytest
 
@@ -106,3 +107,19 @@ def test_format_record_rejects_a_short_buffer(pg):
     buf = ctypes.create_string_buffer(8)
     rc = pg.lib.pg_format_record(buf, 8, 15234, 22.5, 1000003, 503, 2190, 7342)
     assert rc == -1 and "too small" in pg.lib.pg_last_error().decode()
+
+
+def test_package_without_its_library_refuses_to_import(tmp_path):
+    """No CPU fallback: a package copy whose libprimegap.so is absent raises on import."""
+    import shutil
+    pkg = tmp_path / "pkg"
+    shutil.copytree(ROOT / "prime-gap-gpu_b200", pkg, ignore=shutil.ignore_patterns("build", "__pycache__"))
+    code = ("import importlib.util, sys\n"
+            f"spec = importlib.util.spec_from_file_location('pgcopy', r'{pkg / '__init__.py'}', "
+            f"submodule_search_locations=[r'{pkg}'])\n"
+            "m = importlib.util.module_from_spec(spec)\n"
+            "sys.modules['pgcopy'] = m\n"
+            "spec.loader.exec_module(m)\n")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True)
+    assert r.returncode != 0
+    assert "ImportError" in r.stderr and "libprimegap.so is missing" in r.stderr
