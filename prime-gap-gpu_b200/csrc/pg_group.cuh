@@ -183,10 +183,12 @@ __device__ __forceinline__ void gmac_row(uint32_t (&E)[PH], uint32_t (&H)[PH], i
 // pairing of every word and cost moves on every product): row w
 // of a source lane's LT rows works at offset w, so every index is a
 // compile-time constant and every product is one fused 64-bit multiply-add;
-// after the LT rows the window is moved back by LT words.  A lane sends the
-// word leaving its bottom (E + H, up to 33 bits) to the lane below, which adds
-// it LT words up; in lane 0 that word is 0 mod 2^32 (the Montgomery step) and
-// only its carry stays, in c0, for the next bottom word.
+// after the LT rows the window is moved back by LT words.  The word leaving a
+// lane's bottom is E + H plus the carry kept from the previous bottom word;
+// its low 32 bits go to the lane below, which adds them LT words up, and its
+// carry (one bit) stays in the lane, in c0, for its next bottom word (the
+// same position, so one shuffle per row carries the hand-down).  In lane 0
+// the low word is 0 mod 2^32 (the Montgomery step) and only the carry stays.
 template <int T, int LT>
 __device__ __forceinline__ void gmont_mul(const Group<T> &G, uint32_t (&r)[LT], const uint32_t (&a)[LT],
                                            const uint32_t (&b)[LT], const uint32_t (&n)[LT], uint32_t ninv) {
@@ -194,7 +196,7 @@ __device__ __forceinline__ void gmont_mul(const Group<T> &G, uint32_t (&r)[LT], 
     uint32_t E[PH], H[PH];
 #pragma unroll
     for (int k = 0; k < PH; k++) E[k] = H[k] = 0;
-    uint32_t c0 = 0;  // lane 0: carry into the bottom word
+    uint32_t c0 = 0;  // carry into the lane's bottom word
     const bool bottom = G.gl == 0, top = G.gl == T - 1;
 #pragma unroll 1
     for (int src = 0; src < T; src++) {
@@ -210,22 +212,19 @@ __device__ __forceinline__ void gmont_mul(const Group<T> &G, uint32_t (&r)[LT], 
             // the bottom word leaves: 0 mod 2^32 in lane 0 (its carry stays),
             // handed to the lane below elsewhere
             uint32_t lo = add_cc(E[w], H[w]);
-            uint32_t hi = addc(0u, 0u);
-            if (bottom) {
-                (void)add_cc(lo, c0);
-                c0 = addc(hi, 0u);
-            }
+            const uint32_t hi = addc(0u, 0u);
+            lo = add_cc(lo, c0);
+            c0 = addc(hi, 0u);
             uint32_t rlo = __shfl_down_sync(G.gmask, lo, 1);
-            uint32_t rhi = __shfl_down_sync(G.gmask, hi, 1);
-            if (top) rlo = rhi = 0;
+            if (top) rlo = 0;
             const int P = w + LT;
             if ((P & 1) == 0) {
                 E[P] = add_cc(E[P], rlo);
-                E[P + 1] = addc_cc(E[P + 1], rhi);
+                E[P + 1] = addc_cc(E[P + 1], 0u);
                 E[P + 2] = addc(E[P + 2], 0u);
             } else {
                 H[P] = add_cc(H[P], rlo);
-                H[P + 1] = addc_cc(H[P + 1], rhi);
+                H[P + 1] = addc_cc(H[P + 1], 0u);
                 H[P + 2] = addc(H[P + 2], 0u);
             }
         }
@@ -237,12 +236,12 @@ __device__ __forceinline__ void gmont_mul(const Group<T> &G, uint32_t (&r)[LT], 
         }
     }
     // the slice (positions 0 .. LT-1) and what lies above it (LT, LT+1), plus
-    // lane 0's last carry at position 0
+    // the lane's last bottom carry at position 0
     uint32_t R[LT + 2];
     R[0] = add_cc(E[0], H[0]);
 #pragma unroll
     for (int k = 1; k < LT + 2; k++) R[k] = (k + 1 < LT + 2) ? addc_cc(E[k], H[k]) : addc(E[k], H[k]);
-    R[0] = add_cc(R[0], bottom ? c0 : 0u);
+    R[0] = add_cc(R[0], c0);
 #pragma unroll
     for (int k = 1; k < LT + 2; k++) R[k] = (k + 1 < LT + 2) ? addc_cc(R[k], 0u) : addc(R[k], 0u);
     const uint64_t spill = ((uint64_t)R[LT + 1] << 32) | R[LT];
