@@ -98,7 +98,7 @@ class ClockSampler:
 
 # ------------------------------------------------------------- CPU baseline
 
-def cpu_reference_estimate(threads: int, rows_per_thread: int = 1, seed: int = 1) -> dict:
+def cpu_reference_estimate(threads: int, rows_per_thread: int = 1, seed: int = 1, job=None) -> dict:
     """m/sec of the reference's CPU path on this host, from a bounded sample.
 
     The path is the reference's sieve -- one row per X across every m of the
@@ -109,7 +109,8 @@ def cpu_reference_estimate(threads: int, rows_per_thread: int = 1, seed: int = 1
     rest are whole-row composites), scaled to all such rows; the PRP tests
     per m measured by the oracle's search on `threads` sampled m; the time of
     one GMP strong base-2 test measured on a batch of candidates of the
-    workload's size.
+    workload's size.  `job`: an oracle job of the workload to reuse (its
+    table set-up is not part of the measured path either way).
     """
     import random
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -117,7 +118,9 @@ def cpu_reference_estimate(threads: int, rows_per_thread: int = 1, seed: int = 1
     W = WORKLOAD
     rng = random.Random(seed)
     t0 = time.perf_counter()
-    job = O.Job(W["p"], W["d"], W["sl"], W["max_prime"], threads=threads)
+    own = job is None
+    if own:
+        job = O.Job(W["p"], W["d"], W["sl"], W["max_prime"], threads=threads)
     setup_s = time.perf_counter() - t0
     sly = W["sl"] // 2
     kprimes = [q for q in range(3, W["p"] + 1, 2) if all(q % r for r in range(3, int(q ** 0.5) + 1, 2))
@@ -146,7 +149,8 @@ def cpu_reference_estimate(threads: int, rows_per_thread: int = 1, seed: int = 1
     per_test = t_prp * threads / len(cands)          # seconds of one core per test
     prp_s = len(ms_all) * tests_per_m * per_test / threads
     total = sieve_s + prp_s
-    job.close()
+    if own:
+        job.close()
     return {"value": len(ms_all) / total, "unit": "m/s", "cores": threads, "kind": "port", "cpu": cpu_model(),
             "sample": (f"{R} of {len(real)} sieve rows (X coprime to K) over all {len(ms_all)} m, "
                        f"scaled; PRP tests/m from the oracle search of {len(sample_ms)} m "
@@ -338,12 +342,17 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
 
 def run_reference(args) -> dict:
     threads = host_threads()
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O  # the CPU restatement of the reference path
+    W = WORKLOAD
+    job = O.Job(W["p"], W["d"], W["sl"], W["max_prime"], threads=threads)
     vals, last = [], None
     for i in range(args.warmup + args.steps):
-        est = cpu_reference_estimate(threads, seed=i + 1)
+        est = cpu_reference_estimate(threads, seed=i + 1, job=job)
         if i >= args.warmup:
             vals.append(est["value"])
             last = est
+    job.close()
     v = statistics.median(vals)
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "m/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
@@ -459,7 +468,7 @@ def run_serve(args) -> dict:
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form A/B")
