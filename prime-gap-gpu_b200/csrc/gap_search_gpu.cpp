@@ -200,7 +200,8 @@ struct Engine {
 // The records and counts of one range of --minc m.
 struct RangeOut {
     std::vector<std::string> lines;
-    uint64_t m = 0, tests = 0, ext = 0;
+    uint64_t m = 0, tests = 0, ext = 0, batches = 0;
+    double dev_ms = 0;  // device time of the range's calls
     bool whole = true;  // false when a second Ctrl-C stopped it part-way
     bool done = false;
 };
@@ -235,6 +236,8 @@ static int search_range(Engine &e, const Config &c, uint64_t chunk, uint64_t m_s
         out.m += st.m_count;
         out.tests += st.prp_tests;
         out.ext += st.extended_sides;
+        out.batches++;
+        out.dev_ms += st.total_ms;
         for (uint64_t i = 0; i < st.m_count; i++) {
             const uint64_t gap = (uint64_t)e.prev[pd.buf][i] + e.next[pd.buf][i];
             const double merit = pg_merit(e.info.k_log, e.ms[pd.buf][i], gap);
@@ -339,7 +342,8 @@ int main(int argc, char **argv) {
     char fname[64];
     snprintf(fname, sizeof fname, "records_%u.txt", c.p);
     FILE *rec = fopen(fname, "a");
-    uint64_t total_m = 0, total_tests = 0, total_primes = 0, total_ext = 0;
+    uint64_t total_m = 0, total_tests = 0, total_primes = 0, total_ext = 0, total_batches = 0;
+    double total_dev_s = 0;
     const auto t0 = std::chrono::steady_clock::now();
     // Ranges are handed to the devices in order; each range's records are
     // printed, and the progress file advanced, in range order.
@@ -387,6 +391,8 @@ int main(int argc, char **argv) {
         total_tests += out.tests;
         total_primes += 2 * out.m;
         total_ext += out.ext;
+        total_batches += out.batches;
+        total_dev_s += out.dev_ms / 1e3;
         contiguous = contiguous && out.whole;
         if (contiguous && !c.resume.empty()) {  // the range is done: record where the next one starts
             const std::string tmp = c.resume + ".tmp";
@@ -401,10 +407,19 @@ int main(int argc, char **argv) {
         if (c.verbose >= 1) {
             const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
             printf("\nGPU Timings (%.0f seconds):\n", c.show_timing ? secs : 0.0);
+            // the field names of the reference's print_stats (gap_search_gpu.cpp:138-175); its CPU
+            // pipeline's fields (waiting 4 sieve, filling batches, results, batch fill) have no
+            // counterpart here, and overflowed sides continue on the device
             printf("\tm               : %llu (%.0f/sec)\n", (unsigned long long)total_m, total_m / secs);
+            printf("\tm processed     : %llu (%.0f/sec)\n", (unsigned long long)total_m, total_m / secs);
             printf("\ttotal tests     : %llu (%.1f%% prime) (%.0f/sec)\n", (unsigned long long)total_tests,
                    total_tests ? 100.0 * total_primes / total_tests : 0.0, total_tests / secs);
-            printf("\tpast sl         : %llu sides (continued on the device)\n\n", (unsigned long long)total_ext);
+            printf("\ttotal batches   : %llu (%.5f secs/batch)\n", (unsigned long long)total_batches,
+                   total_batches ? secs / total_batches : 0.0);
+            printf("\trunning on gpu  : %.1f seconds (%.1f%%)\n", total_dev_s,
+                   secs > 0 ? 100.0 * total_dev_s / (secs * ndev) : 0.0);
+            printf("\toverflowed      : %llu (%.1f%% of sides, continued on the device)\n\n",
+                   (unsigned long long)total_ext, total_m ? 100.0 * total_ext / (2.0 * total_m) : 0.0);
         }
     }
     for (auto &t : threads) t.join();
