@@ -90,6 +90,7 @@ struct Placed {
 struct SlotState {
     Slot s;
     std::vector<Placed> placed;
+    std::vector<const Tables *> tabs;  // table sets the launch reads
     bool inflight = false;
     uint64_t seq = 0;
 };
@@ -162,6 +163,15 @@ struct pg_server {
         cv_done.notify_all();
     }
 
+    // A launch in flight may still read a table set whose requests are all
+    // done (one failed while another of its windows was running): such a
+    // set is not evicted until the launch has finished.
+    bool read_in_flight(const Tables *T) const {
+        for (const auto &ss : slot)
+            if (ss.inflight && std::find(ss.tabs.begin(), ss.tabs.end(), T) != ss.tabs.end()) return true;
+        return false;
+    }
+
     void evict(std::map<TableKey, TableEntry>::iterator it) {
         for (auto &kv : it->second.jobs) pg_job_destroy(kv.second);
         tables.erase(it);  // the last reference frees the device tables
@@ -216,7 +226,8 @@ struct pg_server {
                 while (resident() + need > prm.hbm_budget) {  // evict idle sets, oldest use first
                     auto victim = tables.end();
                     for (auto t = tables.begin(); t != tables.end(); ++t)
-                        if (t->second.users == 0 && (victim == tables.end() || t->second.last_use < victim->second.last_use))
+                        if (t->second.users == 0 && !read_in_flight(t->second.T.get()) &&
+                            (victim == tables.end() || t->second.last_use < victim->second.last_use))
                             victim = t;
                     if (victim == tables.end()) break;
                     evict(victim);
@@ -283,6 +294,7 @@ struct pg_server {
         Slot &s = ss.s;
         slot_reset(s);
         ss.placed.clear();
+        ss.tabs.clear();
         uint32_t layout = 0;
         for (uint64_t id : order) {
             const Request &r = reqs.at(id);
@@ -312,6 +324,8 @@ struct pg_server {
                 }
                 const uint32_t nm = s.nm - m_off;
                 ss.placed.push_back(Placed{r.id, m_off, nm, r.nm_assigned});
+                if (std::find(ss.tabs.begin(), ss.tabs.end(), r.job->T.get()) == ss.tabs.end())
+                    ss.tabs.push_back(r.job->T.get());
                 r.nm_assigned += nm;
                 r.next_m += inc;
                 r.windows++;
@@ -335,8 +349,11 @@ struct pg_server {
         return true;
     }
 
-    // Fails the requests of a launch that hit a device error.
+    // Fails the requests of a launch that hit an error; whatever of it was
+    // enqueued has finished before the slot counts as idle.
     void fail_launch(SlotState &ss, int rc, const std::string &err) {
+        cudaStreamSynchronize(ss.s.st);
+        cudaGetLastError();
         for (const Placed &pl : ss.placed) {
             auto it = reqs.find(pl.id);
             if (it != reqs.end()) finish(it->second, rc, err);
