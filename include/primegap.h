@@ -194,7 +194,10 @@ int pg_search(pg_job *job, uint64_t m_start, uint64_t m_inc, int form,
  * For each of the n numbers at d_numbers (n rows of `words` LE uint32, device
  * memory) writes to d_steps[i] the smallest k < max_steps such that
  * d_numbers[i] + 2k passes the strong base-2 test, or 0xFFFFFFFF if none
- * does (even numbers and numbers below 3 give 0xFFFFFFFF).  Enqueued on
+ * does (even numbers and numbers below 3 give 0xFFFFFFFF).  Every candidate
+ * d_numbers[i] + 2k is tested at full width for words < 48; for words = 48 a
+ * candidate that no longer fits in 48 words (d_numbers[i] within 2*max_steps
+ * of 2^1536) is skipped, never reported.  Enqueued on
  * `stream` (a cudaStream_t; NULL = the legacy default stream) of the current
  * device; returns without waiting.
  *
@@ -203,6 +206,9 @@ int pg_search(pg_job *job, uint64_t m_start, uint64_t m_inc, int form,
  * library holds until the process exits.  The first call on each device
  * looks up that array's device address (cudaGetSymbolAddress) with the
  * device current: make the first call on a device before any stream capture.
+ * The address is kept for the life of the process: after cudaDeviceReset (or
+ * any teardown of the device's primary context) the module may load elsewhere,
+ * so do not call this function on that device again in the same process.
  * n above PG_NOALLOC_MAX_N is rejected (PG_ERR_ARG), words above 48
  * (PG_ERR_UNSUPPORTED).  Every call shares the array and clears it before
  * use, so calls that can overlap on the GPU (other streams, other host

@@ -38,9 +38,12 @@ __constant__ uint16_t c_trial[64] = {3,   5,   7,   11,  13,  17,  19,  23,  29,
                                      179, 181, 191, 193, 197, 199, 211, 223, 227, 229, 233, 239, 241,
                                      251, 257, 263, 269, 271, 277, 281, 283, 293, 307, 311, 313};
 
-// x + 2k as L words (x has `words` words, zero-extended)
+// x + 2k as L words (x has `words` words, zero-extended).  Returns true when
+// the sum carries out of word L-1, i.e. x + 2k does not fit in L words; the
+// host picks L > words whenever a layout that wide exists, so this happens
+// only for 48-word numbers within 2 * max_steps of 2^1536.
 template <int L>
-__device__ __forceinline__ void load_plus(const uint32_t *__restrict__ row, uint32_t words, uint32_t k,
+__device__ __forceinline__ bool load_plus(const uint32_t *__restrict__ row, uint32_t words, uint32_t k,
                                           uint32_t (&x)[L]) {
 #pragma unroll
     for (int w = 0; w < L; w++) x[w] = ((uint32_t)w < words) ? row[w] : 0u;
@@ -48,7 +51,8 @@ __device__ __forceinline__ void load_plus(const uint32_t *__restrict__ row, uint
     x[0] = add_cc(x[0], (uint32_t)add);
     x[1] = addc_cc(x[1], (uint32_t)(add >> 32));
 #pragma unroll
-    for (int w = 2; w < L; w++) x[w] = (w + 1 < L) ? addc_cc(x[w], 0u) : addc(x[w], 0u);
+    for (int w = 2; w < L; w++) x[w] = addc_cc(x[w], 0u);
+    return addc(0u, 0u) != 0u;
 }
 
 // true when x has a factor among the first 64 odd primes (and x is not that prime)
@@ -104,8 +108,8 @@ __global__ void __launch_bounds__(128) k_next_prime_noalloc(const uint32_t *__re
                     k = (uint32_t)(t / n);
                     i = (uint32_t)(t - (unsigned long long)k * n);
                     if (*(volatile const uint32_t *)&found[i] >= k) {
-                        load_plus<L>(nums + (size_t)i * words, words, k, x);
-                        have = !trial_composite<L>(x);
+                        const bool wrapped = load_plus<L>(nums + (size_t)i * words, words, k, x);
+                        have = !wrapped && !trial_composite<L>(x);
                     }
                 }
             }
@@ -164,8 +168,12 @@ extern "C" int pg_next_prime_noalloc(const uint32_t *d_numbers, uint32_t n, uint
     }
     if (words == 0) return na_fail(PG_ERR_ARG, "words must be > 0");
     if (max_steps == 0) return na_fail(PG_ERR_ARG, "max_steps must be > 0");
-    const uint32_t L = pick_limbs(words);
-    if (words > 48 || L == 0 || L > 48) return na_fail(PG_ERR_UNSUPPORTED, "words above the compiled limit of 48");
+    if (words > 48) return na_fail(PG_ERR_UNSUPPORTED, "words above the compiled limit of 48");
+    // a layout with a spare word holds every x + 2k (2k < 2^33); only 48-word
+    // numbers run without one, and their candidates past 2^1536 are skipped
+    uint32_t L = words < 48 ? pick_limbs(words + 1) : 0;
+    if (L == 0 || L > 48) L = pick_limbs(words);
+    if (L == 0 || L > 48) return na_fail(PG_ERR_UNSUPPORTED, "words above the compiled limit of 48");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return na_fail(PG_ERR_CUDA, "cudaGetDevice", e);

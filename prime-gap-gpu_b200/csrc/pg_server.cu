@@ -350,10 +350,20 @@ struct pg_server {
     }
 
     // Fails the requests of a launch that hit an error; whatever of it was
-    // enqueued has finished before the slot counts as idle.
-    void fail_launch(SlotState &ss, int rc, const std::string &err) {
-        cudaStreamSynchronize(ss.s.st);
-        cudaGetLastError();
+    // enqueued has finished before the slot counts as idle.  The server lock
+    // is released while the stream drains, so submit / wait / next_done
+    // callers do not block on device time; only this worker thread touches
+    // the slot meanwhile.
+    void fail_launch(std::unique_lock<std::mutex> &lk, SlotState &ss, int rc, std::string err) {
+        lk.unlock();
+        const cudaError_t es = cudaStreamSynchronize(ss.s.st);
+        const cudaError_t el = cudaGetLastError();
+        lk.lock();
+        const cudaError_t extra = es != cudaSuccess ? es : el;
+        if (extra != cudaSuccess) {
+            err += "; draining the launch: ";
+            err += cudaGetErrorString(extra);
+        }
         for (const Placed &pl : ss.placed) {
             auto it = reqs.find(pl.id);
             if (it != reqs.end()) finish(it->second, rc, err);
@@ -400,7 +410,7 @@ struct pg_server {
                 ss.seq = ++launch_seq;
                 int rc = slot_enqueue(ss.s, PG_SEARCH_PERSISTENT, PG_SUBMIT_WARPS_PER_SM(prm.warps_per_sm), false);
                 if (rc) {
-                    fail_launch(ss, rc, pg_last_error());
+                    fail_launch(lk, ss, rc, pg_last_error());
                     continue;
                 }
                 ss.inflight = true;
@@ -423,7 +433,7 @@ struct pg_server {
                 const std::string err = rc ? pg_last_error() : "";
                 lk.lock();
                 if (rc)
-                    fail_launch(*oldest, rc, err);
+                    fail_launch(lk, *oldest, rc, err);
                 else
                     deliver(*oldest);
                 bool any = false;

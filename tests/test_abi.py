@@ -123,3 +123,27 @@ def test_package_without_its_library_refuses_to_import(tmp_path):
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True)
     assert r.returncode != 0
     assert "ImportError" in r.stderr and "libprimegap.so is missing" in r.stderr
+
+
+def test_struct_layouts_match_the_header(pg, tmp_path):
+    """Every ctypes mirror of a header struct has the C sizes and field offsets (gcc on the header)."""
+    import ctypes
+    mirrors = {"pg_job_params": pg.JobParams, "pg_job_info": pg.JobInfo, "pg_search_stats": pg.SearchStats,
+               "pg_server_params": pg.ServerParams, "pg_request": pg.Request, "pg_request_info": pg.RequestInfo,
+               "pg_server_stats": pg.ServerStats}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "primegap.h"', "int main(void) {"]
+    for cname, cls in mirrors.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for f, _ in cls._fields_:
+            lines.append(f'printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                         check=True).stdout.splitlines())
+    for cname, cls in mirrors.items():
+        assert int(got[cname]) == ctypes.sizeof(cls), cname
+        for f, _ in cls._fields_:
+            assert int(got[f"{cname}.{f}"]) == getattr(cls, f).offset, f"{cname}.{f}"

@@ -246,8 +246,9 @@ def test_random_shapes_against_gmp(pg, oracle, shape):
     try:
         job = pg.Job(P, d, sl, limit, max_m_inc=m_inc, max_m=m_start + m_inc, tpi=tpi, rounds=rounds)
     except pg.PrimeGapError as e:
-        assert e.code == -3  # no compiled layout of that width for the requested tpi
-        return
+        if e.code != -3:
+            raise
+        pytest.skip(f"no compiled layout for this width with tpi={tpi}: {e}")
     with job:
         res = job.search(m_start, m_inc, form)
     assert len(res.ms) == pg.count_m(m_start, m_inc, d)

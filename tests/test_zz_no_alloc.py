@@ -39,14 +39,20 @@ def _numbers(seed: int, n: int, bits: int) -> list[int]:
 
 
 def _expected(ctx, nums: list[int], words: int, max_steps: int) -> list[int]:
-    """First k < max_steps with nums[i] + 2k passing base 2, via pg_prp_batch."""
+    """First k < max_steps with nums[i] + 2k passing base 2, via pg_prp_batch.
+    At 48 words (the widest layout) candidates of 2^1536 or more are skipped."""
     res = []
+    top = 1 << (32 * words) if words == 48 else None
     for x in nums:
+        ks = [k for k in range(max_steps) if top is None or x + 2 * k < top]
+        if not ks or x % 2 == 0:
+            res.append(NOT_FOUND)
+            continue
         cands = np.stack([np.frombuffer((x + 2 * k).to_bytes(words * 4 + 4, "little"), dtype=np.uint32)
-                          for k in range(max_steps)])
+                          for k in ks])
         passed = ctx.prp_words(cands, rounds=1)
         hit = np.nonzero(passed == 1)[0]
-        res.append(int(hit[0]) if len(hit) and x % 2 == 1 else NOT_FOUND)
+        res.append(ks[int(hit[0])] if len(hit) else NOT_FOUND)
     return res
 
 
@@ -81,3 +87,37 @@ def test_noalloc_rejects_sizes_beyond_the_scratch(pg):
     assert "PG_NOALLOC_MAX_N" in pg.lib.pg_last_error().decode()
     assert f(buf.data_ptr(), 1, 49, 4, buf.data_ptr(), None) == -3
     assert f(buf.data_ptr(), 0, 4, 4, buf.data_ptr(), None) == 0
+
+
+def test_noalloc_full_batch_then_one_step(pg, ctx):
+    """n = PG_NOALLOC_MAX_N (the queue runs to n * max_steps items), checked on
+    a sample against pg_prp_batch; then a call of max_steps 1 right after it,
+    on numbers whose found[] entries the big call filled."""
+    n, words, steps = 65536, 22, 4
+    rng = random.Random(5)
+    nums = [rng.getrandbits(700) | (1 << 699) | 1 for _ in range(n)]
+    got = _run(pg, nums, words, steps)
+    sample = sorted(rng.sample(range(n), 96))
+    assert [got[i] for i in sample] == _expected(ctx, [nums[i] for i in sample], words, steps)
+    assert sum(v != NOT_FOUND for v in got) > n // 100   # ~3.6% of 4-candidate runs hold a prime
+    small = nums[:64]
+    got1 = _run(pg, small, words, 1)
+    assert got1 == _expected(ctx, small, words, 1)
+
+
+@pytest.mark.parametrize("words", [22, 48])
+def test_noalloc_numbers_at_the_top_of_their_width(pg, ctx, words):
+    """Numbers just below 2^(32*words): their candidates carry into a word the
+    input does not have.  Below 48 words the kernel runs a layout with a spare
+    word and tests them at full width (2^704 + 327 is the first prime above
+    2^704); at 48 words they are skipped (no prime lies in 2^1536 - 599 ..
+    2^1536, so every result is 0xFFFFFFFF)."""
+    top = 1 << (32 * words)
+    nums = [top - 2 * j - 1 for j in (0, 1, 5, 40, 150, 299)]
+    steps = 300
+    got = _run(pg, nums, words, steps)
+    assert got == _expected(ctx, nums, words, steps)
+    if words == 22:
+        assert any(v != NOT_FOUND and nums[i] + 2 * v >= top for i, v in enumerate(got))
+    else:
+        assert all(v == NOT_FOUND for v in got)
