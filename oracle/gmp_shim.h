@@ -10,7 +10,10 @@
  * mpz_xxx function is exported as __gmpz_xxx, and mpz_t is a one-element
  * array of {int alloc; int size; mp_limb_t *d;}.  Only the functions the
  * reference calls on its CPU path (gap_common.cpp:60-65, gpu_testing.cu:171,
- * miller_rabin.h:39-54, overflow.cpp:124-168) plus a few helpers are listed.
+ * miller_rabin.h:39-54, overflow.cpp:124-168) plus a few helpers are listed;
+ * oracle/include/gmp.h exposes them under the name <gmp.h> so the reference's
+ * own gap_common.cpp and overflow.cpp compile against them (oracle/Makefile,
+ * target ref).
  */
 #ifndef PG_ORACLE_GMP_SHIM_H
 #define PG_ORACLE_GMP_SHIM_H
@@ -35,7 +38,10 @@ typedef __mpz_struct *mpz_ptr;
 typedef const __mpz_struct *mpz_srcptr;
 
 void __gmpz_init(mpz_ptr);
+void __gmpz_inits(mpz_ptr, ...);
+void __gmpz_init_set(mpz_ptr, mpz_srcptr);
 void __gmpz_clear(mpz_ptr);
+void __gmpz_clears(mpz_ptr, ...);
 void __gmpz_set(mpz_ptr, mpz_srcptr);
 void __gmpz_set_ui(mpz_ptr, unsigned long);
 int __gmpz_set_str(mpz_ptr, const char *, int);
@@ -57,6 +63,7 @@ int __gmpz_prevprime(mpz_ptr, mpz_srcptr);
 int __gmpz_probab_prime_p(mpz_srcptr, int);
 void __gmpz_powm(mpz_ptr, mpz_srcptr, mpz_srcptr, mpz_srcptr);
 void __gmpz_powm_ui(mpz_ptr, mpz_srcptr, unsigned long, mpz_srcptr);
+void __gmpz_ui_pow_ui(mpz_ptr, unsigned long, unsigned long);
 void *__gmpz_export(void *, size_t *, int, size_t, int, size_t, mpz_srcptr);
 void __gmpz_import(mpz_ptr, size_t, int, size_t, int, size_t, const void *);
 size_t __gmpz_sizeinbase(mpz_srcptr, int);
@@ -68,7 +75,10 @@ mp_bitcnt_t __gmpz_scan1(mpz_srcptr, mp_bitcnt_t);
 int __gmpz_tstbit(mpz_srcptr, mp_bitcnt_t);
 
 #define mpz_init __gmpz_init
+#define mpz_inits __gmpz_inits
+#define mpz_init_set __gmpz_init_set
 #define mpz_clear __gmpz_clear
+#define mpz_clears __gmpz_clears
 #define mpz_set __gmpz_set
 #define mpz_set_ui __gmpz_set_ui
 #define mpz_set_str __gmpz_set_str
@@ -90,6 +100,7 @@ int __gmpz_tstbit(mpz_srcptr, mp_bitcnt_t);
 #define mpz_probab_prime_p __gmpz_probab_prime_p
 #define mpz_powm __gmpz_powm
 #define mpz_powm_ui __gmpz_powm_ui
+#define mpz_ui_pow_ui __gmpz_ui_pow_ui
 #define mpz_export __gmpz_export
 #define mpz_import __gmpz_import
 #define mpz_sizeinbase __gmpz_sizeinbase
