@@ -112,6 +112,14 @@ typedef struct {
                               the kernel that steps every X */
     uint32_t tpi;          /* threads per number of the PRP kernels: 0 = automatic (one
                               thread up to 48 words, then groups), 1, or a group size 4 / 8 */
+    double confirm_merit;  /* record confirmation (the double-check of overflow.cpp:164-177):
+                              for every m whose gap has merit > confirm_merit, both primes
+                              must pass confirm_rounds strong bases (2, 3, 5, ...) before the
+                              search returns; a side whose prime fails one is searched on
+                              from its next candidate, so the gap stays exact.  The bulk
+                              search still runs `rounds` bases.  0 = no record confirmation */
+    uint32_t confirm_rounds; /* bases of the record confirmation, 2..16; 0 = 16 */
+    uint32_t pad;
 } pg_job_params;
 
 /* large-prime sieve: 0 = automatic, else force one method */
@@ -171,6 +179,7 @@ typedef struct {
     uint64_t d2h_bytes;       /* device-to-host bytes copied by the call */
     uint32_t graph_launches;  /* CUDA graph launches (the persistent form's window is one graph) */
     uint32_t pad;
+    uint64_t survivors;       /* candidates the sieve left in [-sl, sl], both sides of every m */
 } pg_search_stats;
 
 /* Searches the window: for each m coprime to d (ascending; ms may be NULL)

@@ -78,7 +78,8 @@ class JobParams(ctypes.Structure):
         ("max_prime", ctypes.c_uint64), ("max_m_inc", ctypes.c_uint64), ("max_m", ctypes.c_uint64),
         ("rounds", ctypes.c_uint32), ("small_limit", ctypes.c_uint32),
         ("ext_window", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("search_hits", ctypes.c_uint32),
-        ("tpi", ctypes.c_uint32),
+        ("tpi", ctypes.c_uint32), ("confirm_merit", ctypes.c_double), ("confirm_rounds", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
     ]
 
 
@@ -98,7 +99,7 @@ class SearchStats(ctypes.Structure):
         ("sieve_ms", ctypes.c_double), ("prp_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
         ("search_kernel_ms", ctypes.c_double), ("kernel_launches", ctypes.c_uint64),
         ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
-        ("graph_launches", ctypes.c_uint32), ("pad", ctypes.c_uint32),
+        ("graph_launches", ctypes.c_uint32), ("pad", ctypes.c_uint32), ("survivors", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:
@@ -309,15 +310,25 @@ class SearchResult:
     stats: dict
 
 
+CONFIRM_ROUNDS = 16  # strong bases 2, 3, ..., 53 that both primes of a record pass
+
+
 class Job:
-    """K = P#/d, the sieve tables and the window buffers, resident on one device."""
+    """K = P#/d, the sieve tables and the window buffers, resident on one device.
+
+    confirm_merit: gaps with merit above it have both primes confirmed with
+    confirm_rounds strong bases on the device before a search returns (the
+    record double-check of overflow.cpp:164-177); 0 leaves that to records()."""
 
     def __init__(self, p: int, d: int, sl: int, max_prime: int, max_m_inc: int, max_m: int,
                  rounds: int = 1, small_limit: int = 0, ext_window: int = 0, flags: int = 0,
-                 search_hits: int = 0, tpi: int = 0, ctx: Context | None = None, device: int = 0):
+                 search_hits: int = 0, tpi: int = 0, ctx: Context | None = None, device: int = 0,
+                 confirm_merit: float = 0.0, confirm_rounds: int = 0):
         self.ctx = ctx or Context(device)
         self.params = JobParams(p, d, sl, max_prime, max_m_inc, max_m, rounds, small_limit, ext_window, flags,
-                                search_hits, tpi)
+                                search_hits, tpi, confirm_merit, confirm_rounds, 0)
+        self.confirm_merit = confirm_merit
+        self.confirm_rounds = (confirm_rounds or CONFIRM_ROUNDS) if confirm_merit > 0 else 0
         h = ctypes.c_void_p()
         _check(lib.pg_job_create(self.ctx.handle, ctypes.byref(self.params), ctypes.byref(h)))
         self._h = h
@@ -396,8 +407,28 @@ class Job:
                          for m, a, b in zip(res.ms, res.prev_gap, res.next_gap)])
 
     def records(self, res: SearchResult, min_merit: float) -> list[str]:
-        """Record lines of every gap with merit > min_merit (overflow.cpp:162-188, strict >)."""
-        return records(res, self.k_log, self.p, self.d, min_merit)
+        """Record lines of every gap with merit > min_merit (overflow.cpp:162-188, strict >).
+
+        Every record is confirmed (overflow.cpp:164-177): the search already
+        confirmed both primes of such gaps when the job's confirm_merit is at
+        most min_merit; otherwise both primes are tested here with
+        CONFIRM_ROUNDS strong bases on the device, and a prime that fails
+        raises PrimeGapError (the gap would not be exact: search that window
+        with confirm_merit <= min_merit, which searches on past such a
+        prime)."""
+        lines = records(res, self.k_log, self.p, self.d, min_merit)
+        if lines and not (0 < self.confirm_merit <= min_merit and self.confirm_rounds >= CONFIRM_ROUNDS):
+            ends = []
+            for line in lines:
+                f = line.split()
+                m, prev, gap = int(f[2]), int(f[-1]), int(f[0])
+                ends += [m * self.K - prev, m * self.K - prev + gap]
+            passed = self.ctx.prp(ends, rounds=CONFIRM_ROUNDS)
+            bad = [x for x, v in zip(ends, passed) if v != CONFIRM_ROUNDS]
+            if bad:
+                raise PrimeGapError(-6, f"{len(bad)} record prime(s) failed the {CONFIRM_ROUNDS}-base "
+                                        "confirmation: search with confirm_merit <= min_merit")
+        return lines
 
 
 def records(res: SearchResult, k_log: float, p: int, d: int, min_merit: float) -> list[str]:
@@ -512,7 +543,8 @@ def autotune(p: int, d: int, sl: int, max_prime: int, m_start: int, m_inc: int, 
             return store[key]["knobs"], store[key]["ms"]
     ctx = ctx or Context(0)
     base = JobParams(p, d, sl, max_prime, m_inc, m_start + m_inc, knobs.get("rounds", 1), knobs.get("small_limit", 0),
-                     knobs.get("ext_window", 0), knobs.get("flags", 0), knobs.get("search_hits", 0), knobs.get("tpi", 0))
+                     knobs.get("ext_window", 0), knobs.get("flags", 0), knobs.get("search_hits", 0), knobs.get("tpi", 0),
+                     0.0, 0, 0)
     best = JobParams()
     ms = ctypes.c_double(0)
     _check(lib.pg_autotune(ctx.handle, ctypes.byref(base), m_start, m_inc, ctypes.byref(best), ctypes.byref(ms)))

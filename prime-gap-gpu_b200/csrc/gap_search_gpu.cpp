@@ -16,10 +16,18 @@
 //                      when FILE exists at start (same P, D, MINC), continue from it
 //   --devices A,B,...  one worker per listed CUDA device, each searching whole ranges (the m ranges
 //                      shard with no exchange); records are printed in range order
+//   --confirm-rounds R both primes of every gap with merit > --min-merit pass R strong bases
+//                      (2, 3, 5, ...) on the device before it is printed (default 16; 0 = off):
+//                      the double-check of overflow.cpp:164-177
+//   --spot-check N     GMP re-tests both primes of N m per window with mpz_probab_prime_p(n, 20), as
+//                      the reference spot-checks GPU primes (gpu_testing.cu:125-129, overflow.cpp:117-135);
+//                      libgmp.so.10 is loaded at run time (default 1; 0 = off; skipped with a notice
+//                      when the library is absent)
 // Record lines "{gap} {merit:.3f} {m} * {P}# / {D} - {prev}" go to stdout and
 // are appended to records_{P}.txt.  Ctrl-C once: finish the current window;
 // twice: stop after the current device call; three times: exit(2)
 // (gap_search_gpu.cpp:1050-1069).
+#include <dlfcn.h>
 #include <getopt.h>
 
 #include <atomic>
@@ -60,6 +68,8 @@ struct Config {
     uint32_t warps_per_sm = 6;
     std::string resume;
     std::vector<int> devices;  // --devices; empty = {device}
+    uint32_t confirm_rounds = 16;
+    uint32_t spot_check = 1;
 };
 
 static void show_usage(const char *name) {
@@ -75,7 +85,9 @@ static void show_usage(const char *name) {
     printf("  --warps-per-sm <W>  PRP warps per SM of each of the two windows in flight\n");
     printf("                      (default 6, 0 = as many as fit)\n");
     printf("  --resume <file>     progress file: written after every finished range, read at start\n");
-    printf("  --devices <a,b,..>  search on these CUDA devices, one range per device at a time\n\n");
+    printf("  --devices <a,b,..>  search on these CUDA devices, one range per device at a time\n");
+    printf("  --confirm-rounds <R> strong bases both primes of a record pass (default 16, 0 = off)\n");
+    printf("  --spot-check <N>    m per window whose primes GMP re-tests (default 1, 0 = off)\n\n");
     printf("[OPTIONAL]\n  -q, --quiet\n  -v, --verbose\n  -h, --help\n");
 }
 
@@ -97,7 +109,8 @@ static Config argparse(int argc, char **argv) {
         {"chunk", required_argument, 0, 22},      {"form", required_argument, 0, 23},
         {"rounds", required_argument, 0, 24},     {"device", required_argument, 0, 25},
         {"warps-per-sm", required_argument, 0, 26}, {"resume", required_argument, 0, 27},
-        {"devices", required_argument, 0, 28},
+        {"devices", required_argument, 0, 28},     {"confirm-rounds", required_argument, 0, 29},
+        {"spot-check", required_argument, 0, 30},
         {"quiet", no_argument, 0, 'q'},           {"verbose", no_argument, 0, 'v'},
         {"help", no_argument, 0, 'h'},            {0, 0, 0, 0}};
     Config c;
@@ -141,6 +154,8 @@ static Config argparse(int argc, char **argv) {
                     q = *end == ',' ? end + 1 : end;
                 }
                 break;
+            case 29: c.confirm_rounds = (uint32_t)atoi(optarg); break;
+            case 30: c.spot_check = (uint32_t)atoi(optarg); break;
             default: c.valid = 0;
         }
     }
@@ -160,6 +175,7 @@ static Config argparse(int argc, char **argv) {
     if (c.cpu_fraction < .00001f || c.cpu_fraction > .1f) { c.valid = 0; printf("cpu-fraction must be between .00001 and .1\n"); }
     if (c.cpu_threads < 1 || c.cpu_threads > 159) { c.valid = 0; printf("cpu-threads must be between 1 and 159\n"); }
     if (c.rounds < 1 || c.rounds > 16) { c.valid = 0; printf("rounds must be in 1..16\n"); }
+    if (c.confirm_rounds == 1 || c.confirm_rounds > 16) { c.valid = 0; printf("confirm-rounds must be 0 or in 2..16\n"); }
     return c;
 }
 
@@ -180,6 +196,69 @@ static void on_sigint(int) {
         }                                                                        \
     } while (0)
 
+// GMP spot checks of found primes (the reference re-tests GPU primes with
+// mpz_probab_prime_p(n, 20), gpu_testing.cu:125-129, overflow.cpp:117-135).
+// libgmp is opened at run time so the tool runs without it; only the four
+// public mpz entry points used are declared (GMP exports mpz_xxx as __gmpz_xxx,
+// and an mpz_t is {int alloc; int size; limb *d}).
+struct GmpCheck {
+    struct Mpz {
+        int alloc, size;
+        void *d;
+    };
+    void (*init)(Mpz *) = nullptr;
+    void (*clear)(Mpz *) = nullptr;
+    void (*import_)(Mpz *, size_t, int, size_t, int, size_t, const void *) = nullptr;
+    int (*probab_prime_p)(const Mpz *, int) = nullptr;
+    void *h = nullptr;
+    bool open() {
+        for (const char *name : {"libgmp.so.10", "libgmp.so"}) {
+            h = dlopen(name, RTLD_NOW | RTLD_LOCAL);
+            if (h) break;
+        }
+        if (!h) return false;
+        init = (void (*)(Mpz *))dlsym(h, "__gmpz_init");
+        clear = (void (*)(Mpz *))dlsym(h, "__gmpz_clear");
+        import_ = (void (*)(Mpz *, size_t, int, size_t, int, size_t, const void *))dlsym(h, "__gmpz_import");
+        probab_prime_p = (int (*)(const Mpz *, int))dlsym(h, "__gmpz_probab_prime_p");
+        return init && clear && import_ && probab_prime_p;
+    }
+    // m*K + x (x may be negative) as LE words, then GMP's verdict (> 0: probably prime)
+    int verdict(const std::vector<uint32_t> &K, uint64_t m, int64_t x) const {
+        std::vector<uint32_t> n(K.size() + 3, 0);
+        uint64_t carry = 0;
+        for (size_t i = 0; i < K.size() + 2; i++) {  // n = K * m (m < 2^64: two words)
+            const uint64_t kw = i < K.size() ? K[i] : 0;
+            const unsigned __int128 t = (unsigned __int128)kw * m + carry;
+            n[i] = (uint32_t)t;
+            carry = (uint64_t)(t >> 32);
+        }
+        const uint64_t ax = (uint64_t)(x < 0 ? -x : x);
+        if (x >= 0) {
+            uint64_t c = ax;
+            for (size_t i = 0; i < n.size() && c; i++) {
+                const uint64_t t = (uint64_t)n[i] + (c & 0xffffffffu);
+                n[i] = (uint32_t)t;
+                c = (c >> 32) + (t >> 32);
+            }
+        } else {
+            uint64_t b = ax;
+            for (size_t i = 0; i < n.size() && b; i++) {
+                const uint64_t sub = b & 0xffffffffu;
+                const uint64_t cur = n[i];
+                n[i] = (uint32_t)(cur - sub);
+                b = (b >> 32) + (cur < sub ? 1 : 0);
+            }
+        }
+        Mpz z;
+        init(&z);
+        import_(&z, n.size(), -1, 4, 0, 0, n.data());
+        const int v = probab_prime_p(&z, 20);
+        clear(&z);
+        return v;
+    }
+};
+
 // One device's context and job, with the host buffers of its PG_SEARCH_SLOTS
 // windows in flight.
 struct Engine {
@@ -189,6 +268,9 @@ struct Engine {
     pg_ctx *ctx = nullptr;
     pg_job *job = nullptr;
     pg_job_info info{};
+    std::vector<uint32_t> K;      // K = P#/d, LE words (spot checks)
+    const GmpCheck *gmp = nullptr;
+    uint64_t spot_seq = 0;        // windows finished (picks the spot-checked m)
     std::vector<uint64_t> ms[PG_SEARCH_SLOTS];
     std::vector<uint32_t> prev[PG_SEARCH_SLOTS], next[PG_SEARCH_SLOTS];
     ~Engine() {
@@ -200,7 +282,7 @@ struct Engine {
 // The records and counts of one range of --minc m.
 struct RangeOut {
     std::vector<std::string> lines;
-    uint64_t m = 0, tests = 0, ext = 0, batches = 0;
+    uint64_t m = 0, tests = 0, ext = 0, batches = 0, confirm = 0, spot = 0;
     double dev_ms = 0;  // device time of the range's calls
     bool whole = true;  // false when a second Ctrl-C stopped it part-way
     bool done = false;
@@ -210,6 +292,10 @@ static int make_engine(Engine &e, int device, const pg_job_params &prm, uint64_t
     CHECK(pg_ctx_create(device, &e.ctx));
     CHECK(pg_job_create(e.ctx, &prm, &e.job));
     pg_job_get_info(e.job, &e.info);
+    uint32_t nk = 0;
+    CHECK(pg_job_k_words(e.job, nullptr, &nk));
+    e.K.resize(nk);
+    CHECK(pg_job_k_words(e.job, e.K.data(), &nk));
     for (int k = 0; k < PG_SEARCH_SLOTS; k++) {
         e.ms[k].resize(chunk);
         e.prev[k].resize(chunk);
@@ -235,9 +321,27 @@ static int search_range(Engine &e, const Config &c, uint64_t chunk, uint64_t m_s
                              &st));
         out.m += st.m_count;
         out.tests += st.prp_tests;
+        out.confirm += st.confirm_tests;
         out.ext += st.extended_sides;
         out.batches++;
         out.dev_ms += st.total_ms;
+        // GMP spot checks: both primes of spot_check m spread over the window
+        if (e.gmp && st.m_count) {
+            for (uint32_t q = 0; q < c.spot_check; q++) {
+                const uint64_t i = (e.spot_seq * 7919u + q * 104729u) % st.m_count;
+                const uint64_t m = e.ms[pd.buf][i];
+                const int64_t ends[2] = {(int64_t)e.next[pd.buf][i], -(int64_t)e.prev[pd.buf][i]};
+                for (int64_t x : ends) {
+                    out.spot++;
+                    if (e.gmp->verdict(e.K, m, x) <= 0) {
+                        fprintf(stderr, "\n\nSPOT CHECK FAILED: %llu * %u# / %u %+lld is not prime!\n\n",
+                                (unsigned long long)m, c.p, c.d, (long long)x);
+                        exit(1);
+                    }
+                }
+            }
+            e.spot_seq++;
+        }
         for (uint64_t i = 0; i < st.m_count; i++) {
             const uint64_t gap = (uint64_t)e.prev[pd.buf][i] + e.next[pd.buf][i];
             const double merit = pg_merit(e.info.k_log, e.ms[pd.buf][i], gap);
@@ -306,6 +410,9 @@ int main(int argc, char **argv) {
     prm.max_m_inc = chunk;
     prm.max_m = last_m;
     prm.rounds = c.rounds;
+    // records are confirmed on the device before they are printed
+    prm.confirm_merit = c.confirm_rounds ? std::max(c.min_merit, 1e-9f) : 0.0;
+    prm.confirm_rounds = c.confirm_rounds;
     if (!sl) {
         // log(K) first from a throw-away job with a tiny radius
         pg_ctx *pctx = nullptr;
@@ -324,9 +431,14 @@ int main(int argc, char **argv) {
     }
     prm.sl = sl;
     const size_t ndev = c.devices.size();
+    GmpCheck gmp;
+    const bool have_gmp = c.spot_check && gmp.open();
+    if (c.spot_check && !have_gmp && c.verbose >= 0) printf("spot checks skipped: libgmp.so.10 not found\n");
     std::vector<Engine> eng(ndev);
-    for (size_t k = 0; k < ndev; k++)
+    for (size_t k = 0; k < ndev; k++) {
         if (make_engine(eng[k], c.devices[k], prm, chunk)) return 1;
+        eng[k].gmp = have_gmp ? &gmp : nullptr;
+    }
     const pg_job_info &info = eng[0].info;
     if (c.verbose >= 1) {
         printf("K = %u bits, log(K) = %.2f\n", info.k_bits, info.k_log);
@@ -342,7 +454,8 @@ int main(int argc, char **argv) {
     char fname[64];
     snprintf(fname, sizeof fname, "records_%u.txt", c.p);
     FILE *rec = fopen(fname, "a");
-    uint64_t total_m = 0, total_tests = 0, total_primes = 0, total_ext = 0, total_batches = 0;
+    uint64_t total_m = 0, total_tests = 0, total_primes = 0, total_ext = 0, total_batches = 0, total_confirm = 0,
+             total_spot = 0;
     double total_dev_s = 0;
     const auto t0 = std::chrono::steady_clock::now();
     // Ranges are handed to the devices in order; each range's records are
@@ -392,6 +505,8 @@ int main(int argc, char **argv) {
         total_primes += 2 * out.m;
         total_ext += out.ext;
         total_batches += out.batches;
+        total_confirm += out.confirm;
+        total_spot += out.spot;
         total_dev_s += out.dev_ms / 1e3;
         contiguous = contiguous && out.whole;
         if (contiguous && !c.resume.empty()) {  // the range is done: record where the next one starts
@@ -418,8 +533,11 @@ int main(int argc, char **argv) {
                    total_batches ? secs / total_batches : 0.0);
             printf("\trunning on gpu  : %.1f seconds (%.1f%%)\n", total_dev_s,
                    secs > 0 ? 100.0 * total_dev_s / (secs * ndev) : 0.0);
-            printf("\toverflowed      : %llu (%.1f%% of sides, continued on the device)\n\n",
+            printf("\toverflowed      : %llu (%.1f%% of sides, continued on the device)\n",
                    (unsigned long long)total_ext, total_m ? 100.0 * total_ext / (2.0 * total_m) : 0.0);
+            printf("\tconfirm tests   : %llu (record primes, %u bases each)\n", (unsigned long long)total_confirm,
+                   c.confirm_rounds);
+            printf("\tspot checked    : %llu (GMP mpz_probab_prime_p)\n\n", (unsigned long long)total_spot);
         }
     }
     for (auto &t : threads) t.join();

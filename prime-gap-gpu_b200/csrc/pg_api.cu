@@ -470,6 +470,7 @@ int pg::slot_alloc(Slot &s, uint64_t nm_cap, uint64_t nodd_cap, uint64_t bm_cap,
         (rc = dalloc(b, &s.d_lists, list_cap)) || (rc = dalloc(b, &s.d_counts, S)) || (rc = dalloc(b, &s.d_found, S)) ||
         (rc = dalloc(b, &s.d_kstart, S)) || (rc = dalloc(b, &s.d_knext, S)) || (rc = dalloc(b, &s.d_gaps, S)) ||
         (rc = dalloc(b, &s.d_act0, S)) || (rc = dalloc(b, &s.d_act1, S)) || (rc = dalloc(b, &s.d_redo, S)) ||
+        (rc = dalloc(b, &s.d_conf, S)) ||
         (rc = dalloc(b, &s.d_sc, 1)) || (rc = dalloc(b, &s.d_win, win_cap)))
         return rc;
     PG_CUDA(cudaMallocHost((void **)&s.h_sc, sizeof(Scalars)));
@@ -486,7 +487,7 @@ int pg::slot_alloc(Slot &s, uint64_t nm_cap, uint64_t nodd_cap, uint64_t bm_cap,
 void pg::slot_free(Slot &s) {
     if (s.st) cudaStreamSynchronize(s.st);
     void *ptrs[] = {s.d_ms,   s.d_wid,  s.d_rank, s.d_bitmaps, s.d_lists, s.d_counts, s.d_found, s.d_kstart,
-                    s.d_knext, s.d_gaps, s.d_act0, s.d_act1,    s.d_redo,  s.d_sc,     s.d_win};
+                    s.d_knext, s.d_gaps, s.d_act0, s.d_act1,    s.d_redo,  s.d_conf,   s.d_sc,     s.d_win};
     for (void *p : ptrs) cudaFree(p);
     void *hptrs[] = {s.h_sc, s.h_ms, s.h_wid, s.h_rank, s.h_gaps, s.h_win};
     for (void *p : hptrs) cudaFreeHost(p);
@@ -504,6 +505,7 @@ void pg::slot_reset(Slot &s) {
     s.L = 0;
     s.stride = 0;
     s.ext_window = 0;
+    s.confirm = false;
     s.sst = pg_search_stats{};
 }
 
@@ -554,6 +556,7 @@ int pg::slot_add(Slot &s, pg_job *j, uint64_t m_start, uint64_t m_inc) {
         s.ext_window = p.ext_window;
     }
     s.stride = std::max(s.stride, j->cap);
+    s.confirm = s.confirm || j->win.confirm_rounds >= 2;
     s.nm += w.nm;
     s.nodd += w.nodd;
     s.parts.push_back(w);
@@ -621,6 +624,7 @@ static int run_sieve(Slot &s, const WinPart &w, bool compact) {
     sa.lists = s.d_lists + (size_t)2 * w.m_off * s.stride;
     sa.counts = s.d_counts + (size_t)2 * w.m_off;
     sa.max_count = &s.d_sc->max_count;
+    sa.survivors = &s.d_sc->survivors;
     PG_CUDA(launch_sieve_small(sa, compact, s.st));
     s.sst.kernel_launches++;
     return PG_OK;
@@ -672,11 +676,12 @@ static int enqueue_windows(Slot &s, int form, uint32_t flags) {
     if ((rc = slot_upload(s))) return rc;
     PG_CUDA(record_ev(s.ev[0], s.st));
     PG_CUDA(cudaMemsetAsync(&s.d_sc->max_count, 0, 4, s.st));
+    PG_CUDA(cudaMemsetAsync(&s.d_sc->survivors, 0, 8, s.st));
     for (const WinPart &w : s.parts)
         if ((rc = run_sieve(s, w, true))) return rc;
     PG_CUDA(record_ev(s.ev[1], s.st));
     const uint32_t warps = (uint32_t)s.grid * (PERSIST_THREADS / 32);
-    PG_CUDA(launch_init_search(S, s.d_found, s.d_kstart, s.d_act0, s.d_sc, warps, s.st));
+    PG_CUDA(launch_init_search(S, s.d_found, s.d_kstart, s.d_act0, s.d_conf, s.d_sc, warps, s.st));
     s.sst.kernel_launches++;
     SearchArgs a = base_args(s);
     a.act = s.d_act0;
@@ -768,7 +773,9 @@ int pg::slot_enqueue(Slot &s, int form, uint32_t flags, bool graph) {
 }
 
 // Continues sides without a prime within sl + ext_window on the device with
-// 4x larger extension windows, then reads the timings.
+// 4x larger extension windows; once every side has a prime, confirms the
+// primes of large gaps (windows with confirm_rounds >= 2) and continues the
+// sides whose prime failed from their next candidate.  Then reads the timings.
 int pg::slot_finish(Slot &s) {
     PG_CUDA(cudaStreamSynchronize(s.st));
     if (s.nm == 0) return PG_OK;
@@ -776,7 +783,22 @@ int pg::slot_finish(Slot &s) {
     SearchArgs a = base_args(s);
     uint32_t ext_done = s.ext_window;
     for (int round = 0;; round++) {
-        const uint32_t n_redo = s.h_sc->n_redo;
+        uint32_t n_redo = s.h_sc->n_redo;
+        if (n_redo == 0 && s.confirm) {  // every side resolved: confirm the large gaps
+            SearchArgs c = base_args(s);
+            c.act = s.d_act0;  // 0 .. S-1
+            c.n_act = S;
+            PG_CUDA(cudaMemsetAsync(&s.d_sc->n_redo, 0, 4, s.st));
+            PG_CUDA(launch_confirm(s.L, c, s.d_gaps, s.d_conf, s.d_redo, &s.d_sc->n_redo, &s.d_sc->confirm,
+                                   s.d_kstart, s.st));
+            s.sst.kernel_launches++;
+            PG_CUDA(record_ev(s.ev[2], s.st));
+            PG_CUDA(cudaMemcpyAsync(s.h_gaps, s.d_gaps, (size_t)S * 4, cudaMemcpyDeviceToHost, s.st));
+            PG_CUDA(cudaMemcpyAsync(s.h_sc, s.d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s.st));
+            s.sst.d2h_bytes += 4;
+            PG_CUDA(cudaStreamSynchronize(s.st));
+            n_redo = s.h_sc->n_redo;
+        }
         if (n_redo == 0) break;
         if (round >= 24)
             return fail(PG_ERR_STATE, "pg_search: %u sides unresolved after %u extension positions", n_redo, ext_done);
@@ -815,6 +837,7 @@ int pg::slot_finish(Slot &s) {
     s.sst.total_ms = t_sieve + t_prp;
     s.sst.prp_tests = s.h_sc->tests;
     s.sst.confirm_tests = s.h_sc->confirm;
+    s.sst.survivors = s.h_sc->survivors;
     return PG_OK;
 }
 
@@ -878,6 +901,9 @@ static int job_build(pg_job *j) {
     j->win.kwords = (uint32_t)T.K.size();
     j->win.sly = j->sly;
     j->win.rounds = p.rounds;
+    j->win.k_log = T.k_log;
+    j->win.confirm_merit = p.confirm_merit;
+    j->win.confirm_rounds = p.confirm_merit > 0 ? (p.confirm_rounds ? p.confirm_rounds : 16u) : 0u;
     j->coprime.assign(p.d, 0);
     for (uint32_t r = 0; r < p.d; r++) j->coprime[r] = gcd64(r, p.d) == 1;
     // ---- window capacity
@@ -908,6 +934,10 @@ int pg::job_create(pg_ctx *c, const pg_job_params &p, pg_job **out) {
     if (p.max_prime >= (1ull << 40)) return fail(PG_ERR_ARG, "max_prime must be < 2^40");
     if (p.max_m == 0) return fail(PG_ERR_ARG, "max_m must be set");
     if (p.rounds < 1 || p.rounds > 16) return fail(PG_ERR_ARG, "rounds=%u (1..16)", p.rounds);
+    if (p.confirm_merit < 0 || !(p.confirm_merit == p.confirm_merit))
+        return fail(PG_ERR_ARG, "confirm_merit must be >= 0");
+    if (p.confirm_rounds == 1 || p.confirm_rounds > 16)
+        return fail(PG_ERR_ARG, "confirm_rounds=%u (2..16, 0 = 16)", p.confirm_rounds);
     PG_CUDA(cudaSetDevice(c->device));
     const auto t0 = std::chrono::steady_clock::now();
     pg_job *j = new pg_job();

@@ -123,4 +123,20 @@ cudaError_t launch_finalize(uint32_t L, const SearchArgs &a, uint32_t nsides, ui
     return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_confirm(uint32_t L, const SearchArgs &a, uint32_t *gaps, uint32_t *conf, uint32_t *redo,
+                           uint32_t *n_redo, unsigned long long *confirm_tests, uint32_t *k_start_rw,
+                           cudaStream_t st) {
+    if (a.n_act == 0) return cudaSuccess;
+#define PG_CASE(nl) \
+    if (L == nl) return launch_confirm_t<nl>(a, gaps, conf, redo, n_redo, confirm_tests, k_start_rw, st);
+    PG_LIMB_LIST(PG_CASE)
+#undef PG_CASE
+#define PG_GCASE(t, lt)                                                                                    \
+    if (L == PG_LAYOUT_GROUP(t, (t) * (lt)))                                                               \
+        return glaunch_confirm<t, lt>(a, gaps, conf, redo, n_redo, confirm_tests, k_start_rw, st);
+    PG_GROUP_LIST(PG_GCASE)
+#undef PG_GCASE
+    return cudaErrorInvalidValue;
+}
+
 }  // namespace pg

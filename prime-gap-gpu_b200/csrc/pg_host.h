@@ -93,6 +93,7 @@ struct Slot {
     uint16_t *d_lists = nullptr;
     uint32_t *d_counts = nullptr, *d_found = nullptr, *d_kstart = nullptr, *d_knext = nullptr, *d_gaps = nullptr;
     uint32_t *d_act0 = nullptr, *d_act1 = nullptr, *d_redo = nullptr;
+    uint32_t *d_conf = nullptr;  // per side: the k whose prime passed the record confirmation
     Scalars *d_sc = nullptr;
     WinInfo *d_win = nullptr;
     // pinned host staging
@@ -112,6 +113,7 @@ struct Slot {
     uint32_t L = 0;        // operand layout of every window
     uint32_t stride = 0;   // list stride (largest job capacity)
     uint32_t ext_window = 0;
+    bool confirm = false;  // a window of the slot confirms the primes of its large gaps
     int grid = 0;
     bool busy = false;
     uint64_t ticket = 0;

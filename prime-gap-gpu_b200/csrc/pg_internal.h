@@ -28,9 +28,17 @@ struct WinInfo {
     uint32_t trial_r[TRIAL_PRIMES];    // (-(K mod q)/2) mod q for the trial primes
     uint32_t kwords;
     uint32_t sly;                      // sl / 2; positions Y in [-sly, sly], X = 2Y
-    uint32_t rounds;                   // confirmation: total bases
-    uint32_t pad;
+    uint32_t rounds;                   // confirmation of every accepted prime: total bases
+    uint32_t confirm_rounds;           // record confirmation: total bases (< 2 = off)
+    double k_log;                      // log(K), as the merit's denominator uses it
+    double confirm_merit;              // m whose merit exceeds this get both primes confirmed
 };
+
+// A gap is confirmed when its approximate merit on the device exceeds
+// confirm_merit - CONFIRM_MARGIN: the device log() and the host's differ by a
+// few ulps at most, so every gap the host then finds above confirm_merit has
+// been confirmed.
+constexpr double CONFIRM_MARGIN = 1e-6;
 
 // Arguments of the search kernels (one launch over the sides of one or more
 // windows; the per-side arrays are indexed by the launch's side index).
@@ -65,6 +73,7 @@ struct Scalars {
     unsigned long long next_item;
     unsigned long long tests;
     unsigned long long confirm;
+    unsigned long long survivors;  // list entries the sieve wrote (both sides of every m)
     uint32_t n_redo;
     uint32_t n_out;
     uint32_t max_count;
@@ -93,6 +102,7 @@ struct SieveArgs {
     uint16_t *lists;
     uint32_t *counts;
     uint32_t *max_count;
+    unsigned long long *survivors;
 };
 
 struct LargeArgs {
@@ -132,11 +142,19 @@ cudaError_t launch_compact_active(const uint32_t *act_in, uint32_t n_in, const u
 cudaError_t launch_finalize(uint32_t L, const SearchArgs &a, uint32_t nsides, uint32_t *gaps,
                             uint32_t *redo, uint32_t *n_redo, unsigned long long *confirm_tests,
                             uint32_t *k_start_rw, cudaStream_t st);
+// Record confirmation over the sides a.act[0 .. a.n_act): sides of gaps whose
+// merit exceeds their window's confirm_merit, not yet confirmed at their
+// current k (conf[s]), are tested with bases 3, 5, ... up to confirm_rounds
+// bases in all; failures are reset and queued in redo for another search.
+cudaError_t launch_confirm(uint32_t L, const SearchArgs &a, uint32_t *gaps, uint32_t *conf, uint32_t *redo,
+                           uint32_t *n_redo, unsigned long long *confirm_tests, uint32_t *k_start_rw,
+                           cudaStream_t st);
 cudaError_t launch_iota(uint32_t *out, uint32_t n, cudaStream_t st);
-// found_k = NOT_FOUND, k_start = 0, act = 0..S-1 for S sides; the scalars'
-// queue head and counters = 0, unresolved = S, active_warps = warps
-cudaError_t launch_init_search(uint32_t S, uint32_t *found_k, uint32_t *k_start, uint32_t *act, Scalars *sc,
-                               uint32_t warps, cudaStream_t st);
+// found_k = NOT_FOUND, k_start = 0, act = 0..S-1, conf = NOT_FOUND for S
+// sides; the scalars' queue head and counters = 0, unresolved = S,
+// active_warps = warps
+cudaError_t launch_init_search(uint32_t S, uint32_t *found_k, uint32_t *k_start, uint32_t *act, uint32_t *conf,
+                               Scalars *sc, uint32_t warps, cudaStream_t st);
 cudaError_t launch_imad_peak(int grid, uint32_t iters, uint32_t *sink, cudaStream_t st);
 // records the calling thread's pg_last_error() text (pg_api.cu)
 void set_error(const char *msg);

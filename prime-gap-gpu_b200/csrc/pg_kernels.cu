@@ -616,6 +616,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_sieve_small(const __grid_cons
         a.counts[2 * r] = s_count[0];
         a.counts[2 * r + 1] = s_count[1];
         atomicMax(a.max_count, max(s_count[0], s_count[1]));
+        atomicAdd(a.survivors, (unsigned long long)(s_count[0] + s_count[1]));
     }
 }
 
@@ -662,13 +663,14 @@ __global__ void k_iota(uint32_t *out, uint32_t n) {
     if (i < n) out[i] = i;
 }
 
-__global__ void k_init_search(uint32_t S, uint32_t *found_k, uint32_t *k_start, uint32_t *act, Scalars *sc,
-                              uint32_t warps) {
+__global__ void k_init_search(uint32_t S, uint32_t *found_k, uint32_t *k_start, uint32_t *act, uint32_t *conf,
+                              Scalars *sc, uint32_t warps) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < S) {
         found_k[i] = NOT_FOUND;
         k_start[i] = 0;
         act[i] = i;
+        conf[i] = NOT_FOUND;
     }
     if (i == 0) {
         sc->next_item = 0;
@@ -681,9 +683,9 @@ __global__ void k_init_search(uint32_t S, uint32_t *found_k, uint32_t *k_start, 
     }
 }
 
-cudaError_t launch_init_search(uint32_t S, uint32_t *found_k, uint32_t *k_start, uint32_t *act, Scalars *sc,
-                               uint32_t warps, cudaStream_t st) {
-    k_init_search<<<(S + 255) / 256 + 1, 256, 0, st>>>(S, found_k, k_start, act, sc, warps);
+cudaError_t launch_init_search(uint32_t S, uint32_t *found_k, uint32_t *k_start, uint32_t *act, uint32_t *conf,
+                               Scalars *sc, uint32_t warps, cudaStream_t st) {
+    k_init_search<<<(S + 255) / 256 + 1, 256, 0, st>>>(S, found_k, k_start, act, conf, sc, warps);
     return cudaGetLastError();
 }
 

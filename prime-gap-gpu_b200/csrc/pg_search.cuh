@@ -252,6 +252,53 @@ __global__ void __launch_bounds__(128) k_finalize(const __grid_constant__ Search
     gaps[s] = 2 * Y;
 }
 
+// Record confirmation, one warp per side (the double-check of overflow.cpp:
+// 164-177 done on the device).  The search accepts a prime on one strong
+// base-2 test; a composite that passes it (a base-2 pseudoprime) would end a
+// gap early, while no prime is ever rejected (a prime passes every base and
+// the sieve removes only multiples of its primes).  So a gap is exact once
+// its two ends pass more bases: a side whose gap and partner gap are both
+// known, with merit (prev + next) / (k_log + log m) above its window's
+// confirm_merit, has its prime tested with bases 3, 5, ... (confirm_rounds in
+// all, one base per lane).  A failure resets the side to search again from
+// its next candidate; conf[s] keeps the k confirmed, so a later pass re-tests
+// only sides whose prime changed.
+template <int L>
+__global__ void __launch_bounds__(128) k_confirm(const __grid_constant__ SearchArgs a, uint32_t *gaps, uint32_t *conf,
+                                                 uint32_t *redo, uint32_t *n_redo,
+                                                 unsigned long long *confirm_tests, uint32_t *k_start_rw) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= a.n_act) return;
+    const uint32_t s = a.act[warp];
+    const WinInfo &w = win_of(a, s);
+    const uint32_t k = a.found_k[s];
+    if (w.confirm_rounds < 2 || k == NOT_FOUND || conf[s] == k) return;
+    const uint32_t g = gaps[s], g2 = gaps[s ^ 1u];
+    if (g == 0 || g2 == 0) return;  // the other side is still open: a later pass decides
+    const uint64_t m = a.ms[s >> 1];
+    const double merit = (double)(g + g2) / (w.k_log + log((double)m));
+    if (!(merit > w.confirm_merit - CONFIRM_MARGIN)) return;
+    const uint32_t bases[16] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53};
+    const uint32_t extra = min(w.confirm_rounds, 16u) - 1;
+    bool ok = true;
+    if (lane < extra) {
+        uint32_t x[L];
+        build_candidate<L>(w.K, m, g >> 1, s & 1, x);
+        ok = strong_prp<L>(x, bases[lane + 1]);
+    }
+    const bool all = __all_sync(0xffffffffu, ok);
+    if (lane == 0) {
+        atomicAdd(confirm_tests, (unsigned long long)extra);
+        if (all) {
+            conf[s] = k;
+        } else {
+            a.found_k[s] = NOT_FOUND;
+            gaps[s] = 0;
+            k_start_rw[s] = k + 1;
+            redo[atomicAdd(n_redo, 1u)] = s;
+        }
+    }
+}
 
 // ------------------------------------------------------------ launchers
 
@@ -291,6 +338,15 @@ cudaError_t launch_finalize_t(const SearchArgs &a, uint32_t nsides, uint32_t *ga
     return cudaGetLastError();
 }
 
+template <int L>
+cudaError_t launch_confirm_t(const SearchArgs &a, uint32_t *gaps, uint32_t *conf, uint32_t *redo, uint32_t *n_redo,
+                             unsigned long long *confirm_tests, uint32_t *k_start_rw, cudaStream_t st) {
+    const uint64_t threads = (uint64_t)a.n_act * 32;
+    k_confirm<L><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(a, gaps, conf, redo, n_redo, confirm_tests,
+                                                                    k_start_rw);
+    return cudaGetLastError();
+}
+
 #define PG_DECLARE_LIMBS(L)                                                                                       \
     extern template cudaError_t launch_prp_batch_t<L>(const uint32_t *, uint32_t, uint32_t, uint32_t, int32_t *,  \
                                                       cudaStream_t);                                              \
@@ -298,7 +354,9 @@ cudaError_t launch_finalize_t(const SearchArgs &a, uint32_t nsides, uint32_t *ga
     extern template cudaError_t launch_search_persistent_t<L>(const SearchArgs &, int, cudaStream_t);            \
     extern template cudaError_t launch_search_plain_t<L>(const SearchArgs &, uint32_t *, cudaStream_t);          \
     extern template cudaError_t launch_finalize_t<L>(const SearchArgs &, uint32_t, uint32_t *, uint32_t *,       \
-                                                     uint32_t *, unsigned long long *, uint32_t *, cudaStream_t);
+                                                     uint32_t *, unsigned long long *, uint32_t *, cudaStream_t); \
+    extern template cudaError_t launch_confirm_t<L>(const SearchArgs &, uint32_t *, uint32_t *, uint32_t *,      \
+                                                    uint32_t *, unsigned long long *, uint32_t *, cudaStream_t);
 
 #define PG_INSTANTIATE_LIMBS(L)                                                                                   \
     template cudaError_t launch_prp_batch_t<L>(const uint32_t *, uint32_t, uint32_t, uint32_t, int32_t *,         \
@@ -307,6 +365,8 @@ cudaError_t launch_finalize_t(const SearchArgs &a, uint32_t nsides, uint32_t *ga
     template cudaError_t launch_search_persistent_t<L>(const SearchArgs &, int, cudaStream_t);                   \
     template cudaError_t launch_search_plain_t<L>(const SearchArgs &, uint32_t *, cudaStream_t);                 \
     template cudaError_t launch_finalize_t<L>(const SearchArgs &, uint32_t, uint32_t *, uint32_t *, uint32_t *,  \
-                                              unsigned long long *, uint32_t *, cudaStream_t);
+                                              unsigned long long *, uint32_t *, cudaStream_t);                  \
+    template cudaError_t launch_confirm_t<L>(const SearchArgs &, uint32_t *, uint32_t *, uint32_t *, uint32_t *,  \
+                                             unsigned long long *, uint32_t *, cudaStream_t);
 
 }  // namespace pg

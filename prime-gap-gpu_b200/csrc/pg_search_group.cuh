@@ -221,6 +221,45 @@ __global__ void __launch_bounds__(128) k_finalize_g(const __grid_constant__ Sear
     if (G.gl == 0) gaps[s] = 2 * Y;
 }
 
+// Record confirmation (k_confirm) for lane-group operands: one warp per side,
+// its 32/T groups taking the extra bases in turn.
+template <int T, int LT>
+__global__ void __launch_bounds__(128) k_confirm_g(const __grid_constant__ SearchArgs a, uint32_t *gaps,
+                                                   uint32_t *conf, uint32_t *redo, uint32_t *n_redo,
+                                                   unsigned long long *confirm_tests, uint32_t *k_start_rw) {
+    const Group<T> G;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= a.n_act) return;
+    const uint32_t s = a.act[warp];
+    const WinInfo &w = win_of(a, s);
+    const uint32_t k = a.found_k[s];
+    if (w.confirm_rounds < 2 || k == NOT_FOUND || conf[s] == k) return;
+    const uint32_t g = gaps[s], g2 = gaps[s ^ 1u];
+    if (g == 0 || g2 == 0) return;
+    const uint64_t m = a.ms[s >> 1];
+    const double merit = (double)(g + g2) / (w.k_log + log((double)m));
+    if (!(merit > w.confirm_merit - CONFIRM_MARGIN)) return;
+    const uint32_t bases[16] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53};
+    const uint32_t extra = min(w.confirm_rounds, 16u) - 1;
+    uint32_t x[LT];
+    gbuild_candidate<T, LT>(G, w.K, m, g >> 1, s & 1, x);
+    bool ok = true;
+    for (uint32_t b = G.gb / T; b < extra; b += 32 / T)
+        if (!gstrong_prp<T, LT>(G, x, bases[b + 1])) ok = false;
+    const bool all = __all_sync(0xffffffffu, ok);
+    if (G.lane == 0) {
+        atomicAdd(confirm_tests, (unsigned long long)extra);
+        if (all) {
+            conf[s] = k;
+        } else {
+            a.found_k[s] = NOT_FOUND;
+            gaps[s] = 0;
+            k_start_rw[s] = k + 1;
+            redo[atomicAdd(n_redo, 1u)] = s;
+        }
+    }
+}
+
 // ------------------------------------------------------------ launchers
 
 template <int T, int LT>
@@ -260,6 +299,15 @@ cudaError_t glaunch_finalize(const SearchArgs &a, uint32_t nsides, uint32_t *gap
     return cudaGetLastError();
 }
 
+template <int T, int LT>
+cudaError_t glaunch_confirm(const SearchArgs &a, uint32_t *gaps, uint32_t *conf, uint32_t *redo, uint32_t *n_redo,
+                            unsigned long long *confirm_tests, uint32_t *k_start_rw, cudaStream_t st) {
+    const uint64_t threads = (uint64_t)a.n_act * 32;
+    k_confirm_g<T, LT><<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(a, gaps, conf, redo, n_redo,
+                                                                          confirm_tests, k_start_rw);
+    return cudaGetLastError();
+}
+
 #define PG_GDECLARE(T, LT)                                                                                        \
     extern template cudaError_t glaunch_prp_batch<T, LT>(const uint32_t *, uint32_t, uint32_t, uint32_t,         \
                                                          int32_t *, cudaStream_t);                               \
@@ -267,7 +315,9 @@ cudaError_t glaunch_finalize(const SearchArgs &a, uint32_t nsides, uint32_t *gap
     extern template cudaError_t glaunch_search_persistent<T, LT>(const SearchArgs &, int, cudaStream_t);         \
     extern template cudaError_t glaunch_search_plain<T, LT>(const SearchArgs &, uint32_t *, cudaStream_t);       \
     extern template cudaError_t glaunch_finalize<T, LT>(const SearchArgs &, uint32_t, uint32_t *, uint32_t *,    \
-                                                        uint32_t *, unsigned long long *, uint32_t *, cudaStream_t);
+                                                        uint32_t *, unsigned long long *, uint32_t *, cudaStream_t); \
+    extern template cudaError_t glaunch_confirm<T, LT>(const SearchArgs &, uint32_t *, uint32_t *, uint32_t *,   \
+                                                       uint32_t *, unsigned long long *, uint32_t *, cudaStream_t);
 
 #define PG_GINSTANTIATE(T, LT)                                                                                    \
     template cudaError_t glaunch_prp_batch<T, LT>(const uint32_t *, uint32_t, uint32_t, uint32_t, int32_t *,     \
@@ -276,6 +326,8 @@ cudaError_t glaunch_finalize(const SearchArgs &a, uint32_t nsides, uint32_t *gap
     template cudaError_t glaunch_search_persistent<T, LT>(const SearchArgs &, int, cudaStream_t);                \
     template cudaError_t glaunch_search_plain<T, LT>(const SearchArgs &, uint32_t *, cudaStream_t);              \
     template cudaError_t glaunch_finalize<T, LT>(const SearchArgs &, uint32_t, uint32_t *, uint32_t *,           \
-                                                 uint32_t *, unsigned long long *, uint32_t *, cudaStream_t);
+                                                 uint32_t *, unsigned long long *, uint32_t *, cudaStream_t);    \
+    template cudaError_t glaunch_confirm<T, LT>(const SearchArgs &, uint32_t *, uint32_t *, uint32_t *,          \
+                                                uint32_t *, unsigned long long *, uint32_t *, cudaStream_t);
 
 }  // namespace pg

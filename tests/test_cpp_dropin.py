@@ -62,6 +62,26 @@ def test_cli_records(pg, tmp_path, extra):
     assert (tmp_path / "records_337.txt").read_text().splitlines() == g["records"]
 
 
+@pytest.mark.gpu
+def test_cli_confirms_records_and_spot_checks(pg, tmp_path):
+    """The stats block: every record's primes were confirmed on the device (15 extra bases x 2 sides per
+    record, none past them) and GMP spot-checked found primes; the records are still GMP's."""
+    from conftest import golden
+    g = golden("gaps_P337_d2310.json")
+    cli = pg.LIB_PATH.parent / "gap_search_gpu"
+    out = subprocess.run([str(cli), "-p", "337", "-d", "2310", "--mstart", "10000000", "--minc", "10000",
+                          "--max-prime", "100", "--min-merit", "5", "--sl", "7500", "--ranges", "1",
+                          "--spot-check", "3"], capture_output=True, text=True, cwd=tmp_path, check=True).stdout
+    import re
+    rec = re.compile(r"^\d+ \d+\.\d{3} \d+ \* \d+# / \d+ - \d+$")
+    assert [line for line in out.splitlines() if rec.match(line)] == g["records"]
+    confirm = int(re.search(r"confirm tests\s*: (\d+)", out).group(1))
+    merits = [pg.merit(g["k_log"], m, a + b) for m, a, b in zip(g["ms"], g["prev_gap"], g["next_gap"])]
+    assert confirm == 15 * 2 * sum(x > 5 - 1e-6 for x in merits) and confirm > 0
+    spot = int(re.search(r"spot checked\s*: (\d+)", out).group(1))
+    assert spot == 6  # three m, both primes, one window
+
+
 def test_cli_resume_file_checks(pg, tmp_path):
     """A progress file of another search is refused; a finished one ends the run at once (no device use)."""
     cli = pg.LIB_PATH.parent / "gap_search_gpu"

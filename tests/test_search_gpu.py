@@ -85,6 +85,39 @@ def test_confirmation_rounds(pg, oracle):
     assert res.stats["confirm_tests"] == 2 * 2 * len(res.ms)
 
 
+@pytest.mark.parametrize("form", [0, 1])
+def test_record_confirmation(pg, form):
+    """confirm_merit: both primes of every gap with merit above it pass 16 strong bases before the search
+    returns, and no other prime is tested again.  On the P=337 window (GMP gaps) the confirmation count is
+    15 extra bases x 2 sides for exactly the m whose merit exceeds the threshold; the gaps do not change."""
+    g = golden("gaps_P337_d2310.json")
+    thr = 8.0  # 30 of the window's 2 079 m lie above it (the top merit is 11.7)
+    with _job(pg, g, confirm_merit=thr) as job:
+        res = job.search(g["m_start"], g["m_inc"], form)
+        assert list(res.prev_gap) == g["prev_gap"] and list(res.next_gap) == g["next_gap"]
+        merits = [pg.merit(job.k_log, m, a + b) for m, a, b in zip(g["ms"], g["prev_gap"], g["next_gap"])]
+        over = sum(mer > thr - 1e-6 for mer in merits)
+        assert over > 3
+        assert res.stats["confirm_tests"] == 15 * 2 * over
+        assert job.records(res, g["min_merit"]) == g["records"]
+
+
+@pytest.mark.parametrize("tpi", [1, 8])
+def test_record_confirmation_layouts(pg, oracle, tpi):
+    """The same count on the one-thread and the lane-group kernels (P=503 operands), 8 bases in all."""
+    m_start, m_inc, thr = 1_000_000, 3_000, 9.0  # a few dozen of the 789 m lie above it (the top is 15.2)
+    with pg.Job(503, 2190, 10_000, 20_000_000, max_m_inc=m_inc, max_m=2_000_000, tpi=tpi, confirm_merit=thr,
+                confirm_rounds=8) as job:
+        res = job.search(m_start, m_inc)
+        merits = [pg.merit(job.k_log, int(m), int(a) + int(b))
+                  for m, a, b in zip(res.ms, res.prev_gap, res.next_gap)]
+    with oracle.Job(503, 2190, 10_000, 20_000_000) as oj:
+        prev, nxt = oj.gmp_gaps(res.ms)
+    assert np.array_equal(res.prev_gap, prev) and np.array_equal(res.next_gap, nxt)
+    over = sum(mer > thr - 1e-6 for mer in merits)
+    assert over > 0 and res.stats["confirm_tests"] == 7 * 2 * over
+
+
 def test_search_matches_oracle_search_and_test_count(pg, oracle):
     """Same survivors, same verdicts: the persistent form never tests fewer than the oracle."""
     m_start, m_inc = 1_000_000, 2_000
