@@ -4,22 +4,30 @@ Workload (the single-GPU configuration the metric is quoted on): P=503,
 d=2190, every m in [1,000,000, 1,200,000) coprime to d (52,604 m), candidates
 N = m*503#/2190 + X for X in [-10,000, 10,000] sieved by every prime <= 2e9,
 strong base-2 PRP outward from X = 0 for the previous and the next prime,
-records of merit > 22.  A step is one search of that window (sieve + PRP +
-finalize), the inputs being the window bounds; the prime tables (98 M primes,
-1.18 GB with their K mod p and K^-1 residues) are read again by every step, far
-more than the 126 MB L2, so no L2 flush is needed between steps.  Two windows
-are in flight (two slots of the job, each with its own stream), each window's
-PRP kernel holding at most 6 warps per SM, so one window's tail runs beside the
+records of merit > 22 with both primes confirmed by 16 strong bases.  A step
+is one search of that window (sieve + PRP + finalize + record confirmation),
+the inputs being the window bounds; the prime tables (98 M primes, 1.18 GB
+with their K mod p and K^-1 residues) are read again by every step, far more
+than the 126 MB L2, so no L2 flush is needed between steps.  Two windows are
+in flight (two slots of the job, each with its own stream), each window's PRP
+kernel holding at most 6 warps per SM, so one window's tail runs beside the
 next window's sieve and search; `value` is the m of the K timed windows over
 the device span from the first to the last of them.
 
+Beside the headline the line carries (one GPU only): the other workloads --
+P=337 / 1e8, P=907 / 1e10, a slice of P=3001 / 1e10 with its plain-form A/B
+-- each window searched alone, and a short serving run (64 requests, Poisson
+arrivals at 70% of the measured capacity, p50/p99 latency).
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-  python bench.py --serve      the serving mix instead: capacity and p50/p99 latency
+  python bench.py --serve      the full serving mix instead: capacity and p50/p99 latency
 
 Under torchrun each rank searches its own window of 200,000 m (weak scaling,
 no data-path collective); the reported time is the max over ranks.
-`--impl reference` times the reference's CPU path (the oracle's restatement,
-the reference itself does not build here) on the host cores instead.
+`--impl reference` times the reference's CPU path on the host cores instead:
+its per-X sieve walk up to its overflow cut, the PRP tests of the walk, and
+GMP next / previous prime for the m left at the cut (the oracle's
+restatement; the reference itself needs CGBN and primesieve).
 """
 from __future__ import annotations
 
@@ -98,67 +106,94 @@ class ClockSampler:
 
 # ------------------------------------------------------------- CPU baseline
 
-def cpu_reference_estimate(threads: int, rows_per_thread: int = 1, seed: int = 1, job=None) -> dict:
-    """m/sec of the reference's CPU path on this host, from a bounded sample.
+CPU_FRACTION = 0.005  # the reference's default --cpu-fraction (gap_common.h:47)
 
-    The path is the reference's sieve -- one row per X across every m of the
-    window, every prime <= max_prime (gap_search_gpu.cpp:586-689, corrected)
-    -- followed by GMP strong-PRP tests outward from X = 0 (the overflow path
-    of overflow.cpp:145-160 applied to both sides).  The sample: `threads`
-    X rows of the sieve (only X coprime to K's primes cost anything; the
-    rest are whole-row composites), scaled to all such rows; the PRP tests
-    per m measured by the oracle's search on `threads` sampled m; the time of
-    one GMP strong base-2 test measured on a batch of candidates of the
-    workload's size.  `job`: an oracle job of the workload to reuse (its
-    table set-up is not part of the measured path either way).
+
+class CpuReference:
+    """m/sec of the reference's CPU path for the workload window, on this host.
+
+    The reference (gap_search_gpu.cpp:907-1006) walks the even X > 0 coprime to
+    K's primes outward; for each X it sieves one row across every m of the
+    window by every prime <= max_prime (gap_search_gpu.cpp:570-689, the
+    corrected restatement of the oracle), PRP-tests the survivors among the m
+    still without a next prime, and once fewer than cpu_fraction of the m
+    remain (gap_search_gpu.cpp:976-997) hands those to GMP: next prime from
+    m*K + X_cut + 1, previous prime when the next gap is long
+    (overflow.cpp:145-160).  The PRP tests that the reference runs on its GPU
+    are GMP strong base-2 tests here: this is the CPU path.
+
+    Set-up (not timed): the cut X_cut -- the (1 - cpu_fraction) quantile of the
+    next gaps of `gap_sample` seeded m, from GMP -- and the rows to walk (even X
+    in [2, X_cut] with no factor among K's primes); the PRP tests per m of one
+    side, from the oracle's search of `tests_sample` seeded m (half of its both-
+    sided count).  A step (timed, all host threads): `rows` of the walk's rows
+    sieved across the whole window (a different set each step), scaled to all
+    of them; GMP strong tests on 24 candidates per thread, scaled to the walk's
+    tests; GMP next and previous prime of `tail` of the sampled m with the
+    longest next gaps, scaled to the cpu_fraction of the window left at the cut.
     """
-    import random
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as O  # the CPU restatement (the reference cannot be built in this image)
-    W = WORKLOAD
-    rng = random.Random(seed)
-    t0 = time.perf_counter()
-    own = job is None
-    if own:
-        job = O.Job(W["p"], W["d"], W["sl"], W["max_prime"], threads=threads)
-    setup_s = time.perf_counter() - t0
-    sly = W["sl"] // 2
-    kprimes = [q for q in range(3, W["p"] + 1, 2) if all(q % r for r in range(3, int(q ** 0.5) + 1, 2))
-               and W["d"] % q != 0]
-    real = [y for y in range(-sly, sly + 1) if y != 0 and all(y % q for q in kprimes)]
-    R = max(1, threads * rows_per_thread)
-    ys = [real[(i * len(real)) // R] for i in range(R)]
-    t1 = time.perf_counter()
-    job.sieve_x_rows(W["m_start"], W["m_inc"], ys)
-    t_rows = time.perf_counter() - t1
-    sieve_s = t_rows * len(real) / R
-    ms_all = O.coprime_ms(W["m_start"], W["m_inc"], W["d"])
-    sample_ms = sorted(rng.sample(list(ms_all), threads))
-    t2 = time.perf_counter()
-    _, _, _, tests = job.search(sample_ms, 1)
-    t_search = time.perf_counter() - t2
-    tests_per_m = tests / len(sample_ms)
-    cands = []
-    for _ in range(threads * 24):
-        m = int(rng.choice(ms_all))
-        cands.append(m * job.K + 2 * rng.randrange(-sly, sly) + 1 - 1)
-    cands = [c if c % 2 else c + 1 for c in cands]
-    t3 = time.perf_counter()
-    O.prp_batch(cands, 1, threads)
-    t_prp = time.perf_counter() - t3
-    per_test = t_prp * threads / len(cands)          # seconds of one core per test
-    prp_s = len(ms_all) * tests_per_m * per_test / threads
-    total = sieve_s + prp_s
-    if own:
-        job.close()
-    return {"value": len(ms_all) / total, "unit": "m/s", "cores": threads, "kind": "port", "cpu": cpu_model(),
-            "sample": (f"{R} of {len(real)} sieve rows (X coprime to K) over all {len(ms_all)} m, "
-                       f"scaled; PRP tests/m from the oracle search of {len(sample_ms)} m "
-                       f"({tests_per_m:.1f}/m); {len(cands)} GMP strong base-2 tests timed "
-                       f"({per_test * 1e6:.1f} us/test/core)"),
-            "sieve_seconds_full": sieve_s, "prp_seconds_full": prp_s,
-            "prp_tests_per_sec": len(ms_all) * tests_per_m / total,
-            "sample_seconds": t_rows + t_search + t_prp, "table_setup_seconds": setup_s}
+
+    def __init__(self, threads: int, rows: int = 64, gap_sample: int = 2048, tests_sample: int = 32,
+                 tail: int = 32, seed: int = 1):
+        import random
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O  # the CPU restatement of the reference's path
+        self.O, self.threads, self.rows, self.steps_done = O, threads, rows, 0
+        W = WORKLOAD
+        t0 = time.perf_counter()
+        self.job = O.Job(W["p"], W["d"], W["sl"], W["max_prime"], threads=threads)
+        self.ms_all = O.coprime_ms(W["m_start"], W["m_inc"], W["d"])
+        rng = random.Random(seed)
+        self.rng = rng
+        sample = sorted(rng.sample(list(self.ms_all), gap_sample))
+        _, nxt = self.job.gmp_gaps(sample)
+        order = sorted(range(len(sample)), key=lambda i: int(nxt[i]))
+        self.x_cut = int(nxt[order[int(math.ceil((1 - CPU_FRACTION) * len(sample))) - 1]])
+        self.tail_ms = [sample[i] for i in order[-tail:]]
+        kprimes = [q for q in range(3, W["p"] + 1, 2) if all(q % r for r in range(3, int(q ** 0.5) + 1, 2))
+                   and W["d"] % q != 0]
+        self.walk = [x // 2 for x in range(2, self.x_cut + 1, 2) if all(x % q for q in kprimes)]
+        tsample = sorted(rng.sample(list(self.ms_all), tests_sample))
+        _, _, _, tests = self.job.search(tsample, 1)
+        self.tests_per_m = tests / (2 * len(tsample))  # one side: the reference's walk is next-side only
+        self.setup_s = time.perf_counter() - t0
+
+    def close(self):
+        self.job.close()
+
+    def step(self) -> dict:
+        O, threads, W = self.O, self.threads, WORKLOAD
+        sly = W["sl"] // 2
+        R = min(self.rows, len(self.walk))
+        n_walk = len(self.walk)
+        ys = [self.walk[((i * n_walk) // R + self.steps_done) % n_walk] for i in range(R)]  # each step its own rows
+        self.steps_done += 1
+        t1 = time.perf_counter()
+        self.job.sieve_x_rows(W["m_start"], W["m_inc"], ys)
+        sieve_s = (time.perf_counter() - t1) * n_walk / R
+        cands = [int(self.rng.choice(self.ms_all)) * self.job.K + 2 * self.rng.randrange(1, sly) + 1
+                 for _ in range(threads * 24)]
+        t2 = time.perf_counter()
+        O.prp_batch(cands, 1, threads)
+        per_test = (time.perf_counter() - t2) * threads / len(cands)  # one core's seconds per test
+        n_m = len(self.ms_all)
+        prp_s = n_m * self.tests_per_m * per_test / threads
+        t3 = time.perf_counter()
+        self.job.gmp_gaps(self.tail_ms)
+        per_tail = (time.perf_counter() - t3) * threads / len(self.tail_ms)
+        n_tail = CPU_FRACTION * n_m
+        tail_s = n_tail * per_tail / max(1, min(threads, int(n_tail)))
+        total = sieve_s + prp_s + tail_s
+        return {"value": n_m / total, "unit": "m/s", "cores": threads, "kind": "port", "cpu": cpu_model(),
+                "sample": (f"reference walk of all {n_m} m: {R} of its {n_walk} sieve rows (even X in "
+                           f"[2, {self.x_cut}] coprime to K; X_cut = next-gap quantile {1 - CPU_FRACTION} of "
+                           f"2048 sampled m, the cpu_fraction {CPU_FRACTION} cut) timed across the window and "
+                           f"scaled; {len(cands)} GMP strong base-2 tests timed ({per_test * 1e6:.1f} us/test/core)"
+                           f" x {self.tests_per_m:.1f} tests/m; GMP next+prev prime of {len(self.tail_ms)} tail "
+                           f"m timed, scaled to {n_tail:.0f} m"),
+                "x_cut": self.x_cut, "walk_rows": n_walk, "rows_timed": R,
+                "sieve_seconds_full": sieve_s, "prp_seconds_full": prp_s, "tail_seconds_full": tail_s,
+                "prp_tests_per_sec": n_m * self.tests_per_m / total, "table_setup_seconds": self.setup_s}
 
 
 def cpu_model() -> str:
@@ -186,6 +221,14 @@ def products_per_test(bits: int) -> int:
     return 2 * L * L * (bits + (bits + WINDOW_BITS - 1) // WINDOW_BITS)
 
 
+def kernel_products_per_test(bits: int, limbs: int) -> int:
+    """32x32->64 limb products the PRP kernel executes per strong base-2 test of a `bits`-bit number held in
+    `limbs` words: bits - 1 Montgomery squarings, each L(L+1)/2 cross and diagonal products plus L*L reduction
+    products and L quotient digits (base-2 multiplications are doublings: no products)."""
+    L = limbs
+    return (bits - 1) * (L * (L + 1) // 2 + L * L + L)
+
+
 def traffic_per_launch() -> dict | None:
     f = ROOT / "profiles" / "ncu_traffic.json"
     if f.exists():
@@ -196,18 +239,96 @@ def traffic_per_launch() -> dict | None:
     return None
 
 
+HBM_FALLBACK_GBS = 6650.0  # an earlier copy-bandwidth measurement on this pool's B200s
+
+
+def hbm_peak() -> tuple[float, str]:
+    """HBM copy bandwidth (GB/s) for the sieve's roofline and where it comes from."""
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            v = json.loads(f.read_text()).get("hbm_gbs")
+            if v:
+                return float(v), "measured (MEASURED_PEAKS.json hbm_gbs)"
+        except ValueError:
+            pass
+    return HBM_FALLBACK_GBS, "fallback (6.65 TB/s, an earlier copy measurement on this pool)"
+
+
+def rank_window(rank: int, world: int, m_inc: int = WORKLOAD["m_inc"]) -> tuple[int, int]:
+    """The m window of one rank: ranks search disjoint windows (weak scaling, no data-path exchange)."""
+    if world > len(RANK_STARTS) or not 0 <= rank < world:
+        raise ValueError(f"rank {rank} of {world}: at most {len(RANK_STARTS)} ranks")
+    return RANK_STARTS[rank], m_inc
+
+
+def gather(dist, world: int, mine: dict) -> list[dict]:
+    """Every rank's summary on every rank (the only collective besides the barrier)."""
+    if dist is None or world == 1:
+        return [mine]
+    allr = [None] * world
+    dist.all_gather_object(allr, mine)
+    return allr
+
+
+def aggregate(allr: list[dict]) -> dict:
+    """Whole-job figures from the ranks' summaries: m of all ranks over the slowest rank's device time."""
+    dev_s = max(r["dev_s"] for r in allr)
+    tot_m = sum(r["m"] for r in allr)
+    return {"value": tot_m / dev_s, "dev_s": dev_s, "m": tot_m,
+            "prp_tests_per_sec": sum(r["tests"] for r in allr) / dev_s,
+            "e2e_value": tot_m / max(r["e2e_s"] for r in allr),
+            "launches": sum(r["launches"] for r in allr)}
+
+
+EXTRA = {  # the other workloads, each window searched alone on one GPU
+    "P337": dict(p=337, d=2310, m_start=10_000_000, m_inc=10_000, sl=7_500, max_prime=100_000_000, min_merit=20.0,
+                 windows=5),
+    "P907": dict(p=907, d=210, m_start=1_000_000, m_inc=50_000, sl=18_000, max_prime=10_000_000_000,
+                 min_merit=24.0, windows=3),
+    # a slice of the P=3001 window (its first 600 m): 4 248-bit operands, plain-form A/B on the same m
+    "P3001_slice": dict(p=3001, d=2190, m_start=1, m_inc=600, sl=40_000, max_prime=10_000_000_000,
+                        min_merit=25.0, windows=2, plain=True),
+}
+
+
+def run_config(pg, ctx, w: dict) -> dict:
+    """m/s of one workload window searched alone (device time of the search, inputs resident)."""
+    job = pg.Job(w["p"], w["d"], w["sl"], w["max_prime"], max_m_inc=w["m_inc"], max_m=w["m_start"] + w["m_inc"],
+                 confirm_merit=w["min_merit"], ctx=ctx)
+    try:
+        job.search(w["m_start"], w["m_inc"])  # warm-up (captures the window's graph)
+        st = [job.search(w["m_start"], w["m_inc"]).stats for _ in range(w["windows"])]
+        ms = statistics.median(x["total_ms"] for x in st)
+        n = st[0]["m_count"]
+        out = {"workload": f"P={w['p']} d={w['d']} m in [{w['m_start']:,}, {w['m_start'] + w['m_inc']:,}) coprime "
+                           f"to d, X in [-{w['sl']}, {w['sl']}], primes <= {w['max_prime']:.0e}",
+               "m": n, "ms_per_window": ms, "m_per_sec": n / (ms / 1e3),
+               "prp_tests_per_sec": st[0]["prp_tests"] / (st[0]["total_ms"] / 1e3),
+               "sieve_ms": statistics.median(x["sieve_ms"] for x in st), "limbs": job.info["limbs"],
+               "tpi": job.info["tpi"], "windows_timed": len(st)}
+        if w.get("plain"):
+            pst = [job.search(w["m_start"], w["m_inc"], pg.PG_SEARCH_PLAIN).stats for _ in range(w["windows"])]
+            pms = statistics.median(x["total_ms"] for x in pst)
+            out["plain_ms_per_window"] = pms
+            out["plain_m_per_sec"] = n / (pms / 1e3)
+            out["batched_vs_plain"] = pms / ms
+        return out
+    finally:
+        job.close()
+
+
 def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
     import torch
     import __graft_entry__
     pg = __graft_entry__.load_package()
     torch.cuda.set_device(local_rank)
     W = WORKLOAD
-    m_start = RANK_STARTS[rank]
-    m_inc = args.m_inc
+    m_start, m_inc = rank_window(rank, world, args.m_inc)
     ctx = pg.Context(local_rank)
     t0 = time.perf_counter()
     job = pg.Job(W["p"], W["d"], W["sl"], W["max_prime"], max_m_inc=m_inc, max_m=max(RANK_STARTS) + m_inc,
-                 rounds=1, ctx=ctx)
+                 rounds=1, confirm_merit=W["min_merit"], ctx=ctx)
     setup_s = time.perf_counter() - t0
     imad_peak = ctx.imad_peak()
     dev = torch.device("cuda", local_rank)
@@ -261,11 +382,13 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
     pipelined(args.warmup, False, False)
     res, stats, span_ms, _, _, clocks = pipelined(args.steps, True, False)
     m_count = stats[0]["m_count"]
-    # each window alone (no overlap): the PRP kernel's own time for the roofline
+    # each window alone (no overlap): the PRP kernel's and the sieve's own times for the rooflines
     sstats = synchronous(pg.PG_SEARCH_PERSISTENT, args.steps)
     kern_ms = sum(s["search_kernel_ms"] for s in sstats)
     tests = sum(s["prp_tests"] for s in sstats)
     sync_ms = sum(s["total_ms"] for s in sstats) / args.steps
+    sieve_ms = statistics.median(s["sieve_ms"] for s in sstats)
+    survivors = sstats[0]["survivors"]
     # plain form, same window (the batched-vs-plain A/B)
     plain = None
     if not args.no_plain:
@@ -275,8 +398,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
         plain = {"ms_per_step": pdev / args.steps, "m_per_sec": m_count * args.steps / (pdev / 1e3),
                  "prp_tests": pstats[0]["prp_tests"], "passes": pstats[0]["passes"],
                  "kernel_launches_per_step": pstats[0]["kernel_launches"]}
-    # end to end through the public API: host window in, host gaps + records out
-    _, _, _, e2e_s, nrec, _ = pipelined(args.steps, False, True)
+    # end to end through the public API: host window in, host gaps + confirmed records out
+    _, e2e_stats, _, e2e_s, nrec, _ = pipelined(args.steps, False, True)
     # bit-exactness self-check of this run against the committed GMP fixture
     exact = None
     if rank == 0:
@@ -287,79 +410,106 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
     mine = {"dev_s": span_ms / 1e3, "kern_s": kern_ms / 1e3, "tests": sum(s["prp_tests"] for s in stats),
             "m": m_count * args.steps, "e2e_s": e2e_s, "clocks": clocks, "sync_ms": sync_ms,
             "launches": sum(s["kernel_launches"] for s in stats)}
-    allr = [mine]
-    if dist is not None:
-        allr = [None] * world
-        dist.all_gather_object(allr, mine)
+    allr = gather(dist, world, mine)
     if rank != 0:
+        job.close()
+        ctx.close()
         return None
-    dev_s = max(r["dev_s"] for r in allr)
-    tot_m = sum(r["m"] for r in allr)
+    agg = aggregate(allr)
     bits = (job.K * (m_start + m_inc // 2)).bit_length()
-    ppt = products_per_test(bits)
-    achieved = tests * ppt / (kern_ms / 1e3)           # rank 0's kernel, products/s
+    limbs = job.info["limbs"]
+    ppt_formula = products_per_test(bits)
+    ppt = kernel_products_per_test(bits, limbs)
+    kern_s = kern_ms / 1e3
     peak = imad_peak / 2                               # a 32x32->64 product needs a lo and a hi multiply-add
     tr = traffic_per_launch()
-    roof = {"bound": "imad", "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "G limb-products/s",
-            "frac": achieved / peak, "traffic": tr.get("bytes_per_launch") if tr else None,
+    roof = {"bound": "imad", "achieved": tests * ppt / kern_s / 1e9, "peak": peak / 1e9,
+            "unit": "G limb-products/s", "frac": tests * ppt / kern_s / peak,
+            "frac_formula": tests * ppt_formula / kern_s / peak,
+            "traffic": tr.get("bytes_per_launch") if tr else None,
             "imad_pipe_busy_ncu": tr.get("imad_pipe_busy") if tr else None,
-            "kernel": "k_search_persistent<22>",
-            "work": f"{ppt} limb products per {bits}-bit test (2*L^2*(B+ceil(B/5)), L=ceil(B/32)), "
-                    f"{tests // args.steps} tests per launch",
+            "kernel": f"k_search_persistent<{limbs}>",
+            "work": f"{ppt} limb products per {bits}-bit test ({bits - 1} squarings of {limbs} words: "
+                    f"L(L+1)/2 + L^2 + L each), {tests // args.steps} tests per launch; frac_formula uses the "
+                    f"fixed 2*L^2*(B+ceil(B/5)) = {ppt_formula}",
             "peak_source": "in-run microbenchmark (pg_measure_imad_peak: 32-bit IMAD/s / 2); "
                            "MEASURED_PEAKS.json has no integer-multiply figure"}
+    hbm, hbm_src = hbm_peak()
+    esz = 8 if W["max_prime"] >= 2 ** 32 else 4
+    table_b = job.info["num_primes"] * 3 * esz
+    rows_b = m_count * job.info["words_per_m"] * 4
+    sieve_b = table_b + 2 * rows_b + survivors * 2
+    sieve = {"bound": "hbm", "achieved": sieve_b / (sieve_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+             "frac": sieve_b / (sieve_ms / 1e3) / 1e9 / hbm, "ms_per_window": sieve_ms,
+             "bytes_per_window": sieve_b,
+             "work": f"prime table {table_b / 1e9:.3f} GB ({job.info['num_primes']} primes x 3 x {esz} B, read "
+                     f"once) + rows {rows_b / 1e6:.1f} MB written and read once + {survivors} survivors x 2 B; "
+                     "time = sieve kernels of a window alone (large-prime search, small-prime tiles and lists)",
+             "peak_source": hbm_src}
     line = {
-        "metric": METRIC, "value": tot_m / dev_s, "unit": "m/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
+        "metric": METRIC, "value": agg["value"], "unit": "m/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": agg["dev_s"] * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": workload_name(RANK_STARTS[0], m_inc),
                    "form": f"persistent, {pg.PG_SEARCH_SLOTS} windows in flight"
                            + (f", {args.warps_per_sm} PRP warps per SM per window" if args.warps_per_sm else "")
-                           + (f", draining to {args.drain} lanes per unresolved side" if args.drain else ""),
+                           + (f", draining to {args.drain} lanes per unresolved side" if args.drain else "")
+                           + ", records confirmed with 16 bases",
                    "m_per_gpu_per_step": m_count, "sl": W["sl"], "max_prime": W["max_prime"],
-                   "limbs": job.info["limbs"], "parallelism": f"weak: {world} disjoint m-windows",
+                   "limbs": limbs, "tpi": job.info["tpi"], "parallelism": f"weak: {world} disjoint m-windows",
                    "l2": "inputs larger than L2 (1.18 GB prime tables read every step)"},
-        "prp_tests_per_sec": sum(r["tests"] for r in allr) / dev_s,
+        "prp_tests_per_sec": agg["prp_tests_per_sec"],
         "ms_per_step_one_window_alone": max(r["sync_ms"] for r in allr),
         "setup_seconds": setup_s,
         "bit_exact_vs_gmp_sample": exact,
         "roofline": roof,
-        "e2e": {"value": tot_m / max(r["e2e_s"] for r in allr), "unit": "m/s",
+        "sieve": sieve,
+        "e2e": {"value": agg["e2e_value"], "unit": "m/s",
                 "h2d_bytes_per_step": stats[0]["h2d_bytes"], "d2h_bytes_per_step": stats[0]["d2h_bytes"],
-                "records_per_step": nrec // max(1, args.steps)},
-        "gpu_launches": sum(r["launches"] for r in allr),
+                "records_per_step": nrec / max(1, args.steps),
+                "confirm_tests_per_step": sum(x["confirm_tests"] for x in e2e_stats) / max(1, args.steps)},
+        "gpu_launches": agg["launches"],
         "clocks": allr[0]["clocks"],
     }
     if plain is not None:
         line["plain"] = plain
-        line["batched_vs_plain"] = (tot_m / dev_s) / (plain["m_per_sec"] * world)
-    if world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_reference_estimate(host_threads())
+        line["batched_vs_plain"] = agg["value"] / (plain["m_per_sec"] * world)
     job.close()
-    ctx.close()
+    if world == 1 and not args.no_extra:
+        line["configs"] = {name: run_config(pg, ctx, w) for name, w in EXTRA.items()}
+        ctx.close()
+        line["configs"]["serving"] = run_serve(args, n_jobs=64, compact=True)
+    else:
+        ctx.close()
+    if world == 1 and not args.no_cpu:
+        ref = CpuReference(host_threads())
+        try:
+            line["cpu_baseline"] = ref.step()
+        finally:
+            ref.close()
     return line
 
 
 def run_reference(args) -> dict:
     threads = host_threads()
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as O  # the CPU restatement of the reference path
-    W = WORKLOAD
-    job = O.Job(W["p"], W["d"], W["sl"], W["max_prime"], threads=threads)
+    ref = CpuReference(threads, rows=24)  # 24 rows a step, shifted by one row per step
     vals, last = [], None
-    for i in range(args.warmup + args.steps):
-        est = cpu_reference_estimate(threads, seed=i + 1, job=job)
-        if i >= args.warmup:
-            vals.append(est["value"])
-            last = est
-    job.close()
+    try:
+        for i in range(args.warmup + args.steps):
+            est = ref.step()
+            if i >= args.warmup:
+                vals.append(est["value"])
+                last = est
+    finally:
+        ref.close()
     v = statistics.median(vals)
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "m/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {"workload": workload_name(WORKLOAD["m_start"], WORKLOAD["m_inc"]),
-                       "implementation": "CPU restatement of the reference path (oracle/, GMP 6.3.0); "
-                                         "the reference needs CGBN and primesieve, absent here"},
+                       "implementation": "CPU restatement of the reference path (oracle/, GMP 6.3.0): its per-X "
+                                         "sieve walk to the cpu_fraction cut, GMP PRP tests, GMP next/prev prime "
+                                         "of the tail; the reference needs CGBN and primesieve, absent here"},
             "cpu_baseline": {**{k: last[k] for k in ("unit", "cores", "kind", "sample", "cpu")}, "value": v},
             "e2e": {"value": v, "unit": "m/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "prp_tests_per_sec": last["prp_tests_per_sec"]}
@@ -396,18 +546,22 @@ def serve_requests(n: int = 256, seed: int = SERVE_SEED, limit: int = 1_000_000_
     return out
 
 
-def run_serve(args) -> dict:
+def run_serve(args, n_jobs: int | None = None, compact: bool = False) -> dict:
     """Capacity (all requests queued at once) and latency under Poisson
-    arrivals at 70% of that capacity, through pg_server_*."""
+    arrivals at 70% of that capacity, through pg_server_*.  compact: the
+    short run of the default bench line (n_jobs requests, the server's
+    default launch shape)."""
     import threading
     import numpy as np
     import __graft_entry__
     pg = __graft_entry__.load_package()
-    reqs = serve_requests(args.serve_jobs)
+    reqs = serve_requests(n_jobs or args.serve_jobs)
     classes = sorted({(p, d) for p, d, *_ in reqs})
     max_sl = max(r[2] for r in reqs)
-    with pg.Server(0, max_sl=max_sl, warps_per_sm=args.warps_per_sm, batch_m=args.serve_batch_m,
-                   slots=args.serve_slots) as srv:
+    wps = 0 if compact else args.warps_per_sm
+    batch_m = 0 if compact else args.serve_batch_m
+    slots = 0 if compact else args.serve_slots
+    with pg.Server(0, max_sl=max_sl, warps_per_sm=wps, batch_m=batch_m, slots=slots) as srv:
         # resident tables for every (P, d) first: one small request per class
         warm = [srv.submit(p, d, 1_000, reqs[0][3], 1_000_001, 200) for p, d in classes]
         t = time.perf_counter()
@@ -447,7 +601,7 @@ def run_serve(args) -> dict:
             by_p[str(P)] = {"n": int(sel.sum()), "p50_ms": round(float(np.percentile(lat[sel], 50)), 1),
                             "p99_ms": round(float(np.percentile(lat[sel], 99)), 1)}
     return {
-        "metric": "serving latency p99 (256 gap-search requests, Poisson arrivals at 70% of capacity)",
+        "metric": f"serving latency p99 ({len(reqs)} gap-search requests, Poisson arrivals at 70% of capacity)",
         "value": round(float(np.percentile(lat, 99)), 2), "unit": "ms", "higher_is_better": False,
         "p50_ms": round(float(np.percentile(lat, 50)), 2), "p99_ms": round(float(np.percentile(lat, 99)), 2),
         "mean_ms": round(float(lat.mean()), 2), "latency_by_P": by_p,
@@ -460,8 +614,7 @@ def run_serve(args) -> dict:
         "n_gpus": 1, "data": "synthetic (seeded request mix)",
         "config": {"workload": f"{len(reqs)} requests, P in {{337,503,907}}, d in {{210,2190,2310}}, "
                                "500-20000 m from [1e6,1e9], SL=round(8 ln N), primes <= 1e9",
-                   "seed": SERVE_SEED, "warps_per_sm": args.warps_per_sm,
-                   "batch_m": args.serve_batch_m or 65536, "slots": args.serve_slots or 2},
+                   "seed": SERVE_SEED, "warps_per_sm": wps, "batch_m": batch_m or 65536, "slots": slots or 2},
     }
 
 
@@ -473,6 +626,8 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form A/B")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the other workloads and the short serving run (one GPU only)")
     ap.add_argument("--drain", type=int, default=0, metavar="D",
                     help="let the PRP kernel's warps leave as a window drains, keeping D lanes per "
                          "unresolved side (PG_SUBMIT_DRAIN; 0 = off)")

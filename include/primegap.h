@@ -111,7 +111,7 @@ typedef struct {
                               (default); n > 0 keeps primes expecting >= n hits per window on
                               the kernel that steps every X */
     uint32_t tpi;          /* threads per number of the PRP kernels: 0 = automatic (one
-                              thread up to 48 words, then groups), 1, or a group size 4 / 8 */
+                              thread up to 48 words, then groups), 1, or a group size 4 / 8 / 16 */
     double confirm_merit;  /* record confirmation (the double-check of overflow.cpp:164-177):
                               for every m whose gap has merit > confirm_merit, both primes
                               must pass confirm_rounds strong bases (2, 3, 5, ...) before the
@@ -258,6 +258,34 @@ void *pg_job_stream(pg_job *job, int slot);
  * *best_ms its device time per window.  Builds one job per candidate. */
 int pg_autotune(pg_ctx *ctx, const pg_job_params *base, uint64_t m_start, uint64_t m_inc, pg_job_params *best,
                 double *best_ms);
+
+/* The wider autotuner: the knobs the reference fixes at compile time
+ * (THREADS_PER_INSTANCE, WINDOW_BITS, GPU_BATCH_SIZE, GPU_BATCHES,
+ * gpu_testing.cu:50-62) and their counterparts here, timed on the sample
+ * window [m_start, m_start + m_inc) with PG_SEARCH_SLOTS windows in flight
+ * (the pipelined form callers run), one knob after the other:
+ *   1. threads per number: tpi 0 (automatic), 1, 4, 8, 16 where a compiled
+ *      layout fits;
+ *   2. the small-prime bound of the shared-memory sieve tile: 16384, 65536,
+ *      262144;
+ *   3. the PRP kernel's warps per SM (PG_SUBMIT_WARPS_PER_SM): 0 (all that
+ *      fit), 4, 6, 8, 10, 12;
+ *   4. with PG_TUNE_WINDOW, the m per window: m_inc, m_inc / 2, m_inc / 4.
+ * The exponentiation window has no knob: the base-2 test multiplies by
+ * doublings, never by a table entry.  Each setting runs one warm-up pass and
+ * then `reps` passes (0 = 4) over the sample; m/s is their m over the wall
+ * time.  out->params is *base with the chosen small_limit and tpi. */
+#define PG_TUNE_WINDOW 0x1u
+typedef struct {
+    pg_job_params params;   /* the chosen job parameters */
+    uint32_t warps_per_sm;  /* the chosen PG_SUBMIT_WARPS_PER_SM cap (0 = as many as fit) */
+    uint32_t settings;      /* settings timed */
+    uint64_t window_m;      /* the chosen m per window */
+    double m_per_sec;       /* the chosen setting's m/s, PG_SEARCH_SLOTS windows in flight */
+    double first_m_per_sec; /* m/s of the first setting timed (tpi 0 with base's knobs, no cap) */
+} pg_tune_result;
+int pg_autotune_ex(pg_ctx *ctx, const pg_job_params *base, uint64_t m_start, uint64_t m_inc, uint32_t flags,
+                   uint32_t reps, pg_tune_result *out);
 
 /* ---------------------------------------------------------------- serving
  *

@@ -50,7 +50,7 @@ EXPORTS = (
     "pg_prp_batch", "pg_prp_batch_device",
     "pg_job_create", "pg_job_destroy", "pg_job_get_info", "pg_job_k_words",
     "pg_count_m", "pg_sieve_interval", "pg_search", "pg_merit", "pg_format_record", "pg_next_prime_noalloc",
-    "pg_search_submit", "pg_search_wait", "pg_job_stream", "pg_autotune",
+    "pg_search_submit", "pg_search_wait", "pg_job_stream", "pg_autotune", "pg_autotune_ex",
     "pg_server_create", "pg_server_submit", "pg_server_wait", "pg_server_next_done", "pg_server_get_stats",
     "pg_server_clock", "pg_server_destroy",
 )
@@ -104,6 +104,16 @@ class SearchStats(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [
+        ("params", JobParams), ("warps_per_sm", ctypes.c_uint32), ("settings", ctypes.c_uint32),
+        ("window_m", ctypes.c_uint64), ("m_per_sec", ctypes.c_double), ("first_m_per_sec", ctypes.c_double),
+    ]
+
+
+PG_TUNE_WINDOW = 0x1
 
 
 class ServerParams(ctypes.Structure):
@@ -172,6 +182,7 @@ def _load() -> ctypes.CDLL:
     lib.pg_job_stream.argtypes = [vp, i32]
     lib.pg_autotune.argtypes = [vp, ctypes.POINTER(JobParams), u64, u64, ctypes.POINTER(JobParams),
                                 ctypes.POINTER(ctypes.c_double)]
+    lib.pg_autotune_ex.argtypes = [vp, ctypes.POINTER(JobParams), u64, u64, u32, u32, ctypes.POINTER(TuneResult)]
     lib.pg_merit.restype = ctypes.c_double
     lib.pg_merit.argtypes = [ctypes.c_double, u64, u64]
     lib.pg_format_record.argtypes = [ctypes.c_char_p, ctypes.c_size_t, u64, ctypes.c_double, u64, u32, u32, u64]
@@ -553,6 +564,44 @@ def autotune(p: int, d: int, sl: int, max_prime: int, m_start: int, m_inc: int, 
         store[key] = {"knobs": out, "ms": ms.value}
         cache.write_text(json.dumps(store, indent=1))
     return out, ms.value
+
+
+def autotune_ex(p: int, d: int, sl: int, max_prime: int, m_start: int, m_inc: int, ctx: Context | None = None,
+                windows: bool = False, reps: int = 0, cache: str | pathlib.Path | None = None,
+                **knobs) -> dict:
+    """pg_autotune_ex: threads per number, sieve tile bound, PRP warps per SM and (windows=True) the m per
+    window, timed with PG_SEARCH_SLOTS windows of the sample [m_start, m_start + m_inc) in flight.  Returns
+    {"knobs": job knobs, "warps_per_sm", "window_m", "m_per_sec", "first_m_per_sec", "settings"}.  With
+    `cache`, results are kept in that JSON file keyed by the operand width, threads per number asked, sl and
+    the sample, and reused."""
+    import json
+    key = None
+    if cache is not None:
+        cache = pathlib.Path(cache)
+        store = json.loads(cache.read_text()) if cache.exists() else {}
+        K = 1
+        for q in range(2, p + 1):
+            if all(q % r for r in range(2, int(q ** 0.5) + 1)):
+                K *= q
+        bits = (K // d * (m_start + m_inc)).bit_length()
+        key = (f"bits{bits}/tpi{knobs.get('tpi', 0)}/sl{sl}/P{p}/d{d}/limit{max_prime}/m{m_start}+{m_inc}/"
+               f"win{int(windows)}/" + "/".join(f"{k}={knobs[k]}" for k in sorted(knobs)))
+        if key in store:
+            return store[key]
+    ctx = ctx or Context(0)
+    base = JobParams(p, d, sl, max_prime, m_inc, m_start + m_inc, knobs.get("rounds", 1), knobs.get("small_limit", 0),
+                     knobs.get("ext_window", 0), knobs.get("flags", 0), knobs.get("search_hits", 0),
+                     knobs.get("tpi", 0), knobs.get("confirm_merit", 0.0), knobs.get("confirm_rounds", 0), 0)
+    res = TuneResult()
+    _check(lib.pg_autotune_ex(ctx.handle, ctypes.byref(base), m_start, m_inc, PG_TUNE_WINDOW if windows else 0,
+                              reps, ctypes.byref(res)))
+    out = {"knobs": {k: getattr(res.params, k) for k in JOB_KNOBS}, "warps_per_sm": res.warps_per_sm,
+           "window_m": res.window_m, "m_per_sec": res.m_per_sec, "first_m_per_sec": res.first_m_per_sec,
+           "settings": res.settings}
+    if key is not None:
+        store[key] = out
+        cache.write_text(json.dumps(store, indent=1))
+    return out
 
 
 def merit(k_log: float, m: int, gap: int) -> float:

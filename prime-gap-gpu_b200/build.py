@@ -36,15 +36,18 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+def limbs_header() -> str:
+    """pg_limbs.h with its continued lines joined."""
+    return (CSRC / "pg_limbs.h").read_text().replace("\\\n", " ")
+
+
 def limb_list() -> list[int]:
-    text = (CSRC / "pg_limbs.h").read_text()
-    m = re.search(r"#define PG_LIMB_LIST\(X\)(.*)", text)
+    m = re.search(r"#define PG_LIMB_LIST\(X\)(.*)", limbs_header())
     return [int(v) for v in re.findall(r"X\((\d+)\)", m.group(1))]
 
 
 def group_list() -> list[tuple[int, int]]:
-    text = (CSRC / "pg_limbs.h").read_text()
-    m = re.search(r"#define PG_GROUP_LIST\(X\)(.*)", text)
+    m = re.search(r"#define PG_GROUP_LIST\(X\)(.*)", limbs_header())
     return [(int(a), int(b)) for a, b in re.findall(r"X\((\d+),\s*(\d+)\)", m.group(1))]
 
 

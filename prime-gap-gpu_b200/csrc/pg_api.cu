@@ -1151,6 +1151,124 @@ extern "C" int pg_autotune(pg_ctx *c, const pg_job_params *base, uint64_t m_star
     return PG_OK;
 }
 
+// m/s of `reps` passes over [m_start, m_start + m_inc) in windows of `window`
+// m, PG_SEARCH_SLOTS in flight, after one warm-up pass (wall clock: the
+// windows are device bound)
+static int time_pipelined(pg_job *j, uint64_t m_start, uint64_t m_inc, uint64_t window, uint32_t flags,
+                          uint32_t reps, double *m_per_sec) {
+    const uint64_t nwin = (m_inc + window - 1) / window;
+    uint64_t m_done = 0;
+    bool timing = false;
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<uint64_t> pending;
+    int rc = PG_OK;
+    auto drain_one = [&]() {
+        pg_search_stats st{};
+        const int r = pg_search_wait(j, pending.front(), nullptr, nullptr, nullptr, &st);
+        pending.erase(pending.begin());
+        if (r == PG_OK && timing) m_done += st.m_count;
+        return r;
+    };
+    for (uint32_t it = 0; it < 1 + reps && rc == PG_OK; it++) {
+        if (it == 1) {  // the warm-up pass is done: start the clock
+            while (!pending.empty() && rc == PG_OK) rc = drain_one();
+            if (rc) break;
+            timing = true;
+            t0 = std::chrono::steady_clock::now();
+        }
+        for (uint64_t w = 0; w < nwin && rc == PG_OK; w++) {
+            if (pending.size() == PG_SEARCH_SLOTS) rc = drain_one();
+            if (rc) break;
+            uint64_t t = 0;
+            const uint64_t inc = std::min(window, m_inc - w * window);
+            rc = pg_search_submit(j, m_start + w * window, inc, PG_SEARCH_PERSISTENT, flags, &t);
+            if (rc == PG_OK) pending.push_back(t);
+        }
+    }
+    while (!pending.empty()) {
+        const int r = drain_one();
+        if (rc == PG_OK) rc = r;
+    }
+    if (rc) return rc;
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *m_per_sec = m_done / std::max(secs, 1e-9);
+    return PG_OK;
+}
+
+extern "C" int pg_autotune_ex(pg_ctx *c, const pg_job_params *base, uint64_t m_start, uint64_t m_inc, uint32_t flags,
+                              uint32_t reps, pg_tune_result *out) {
+    if (!c || !base || !out) return fail(PG_ERR_ARG, "pg_autotune_ex: NULL argument");
+    if (m_inc == 0) return fail(PG_ERR_ARG, "pg_autotune_ex: m_inc must be > 0");
+    if (!reps) reps = 4;
+    pg_job_params p = *base;
+    p.max_m_inc = std::max<uint64_t>(p.max_m_inc, m_inc);
+    p.max_m = std::max<uint64_t>(p.max_m, m_start + m_inc);
+    pg_tune_result best{};
+    best.params = p;
+    best.window_m = m_inc;
+    uint32_t settings = 0;
+    // times job parameters q with warps cap w and window size win; keeps the best
+    auto trial = [&](const pg_job_params &q, uint32_t w, uint64_t win) -> int {
+        pg_job *j = nullptr;
+        int rc = pg_job_create(c, &q, &j);
+        if (rc) return rc;
+        double v = 0;
+        rc = time_pipelined(j, m_start, m_inc, win, PG_SUBMIT_WARPS_PER_SM(w), reps, &v);
+        pg_job_destroy(j);
+        if (rc) return rc;
+        if (settings++ == 0) best.first_m_per_sec = v;
+        if (v > best.m_per_sec) {
+            best.m_per_sec = v;
+            best.params = q;
+            best.warps_per_sm = w;
+            best.window_m = win;
+        }
+        return PG_OK;
+    };
+    // 1. threads per number
+    const uint32_t tpis[] = {0, 1, 4, 8, 16};
+    for (uint32_t t : tpis) {
+        pg_job_params q = p;
+        q.tpi = t;
+        const int rc = trial(q, 0, m_inc);
+        if (rc == PG_ERR_UNSUPPORTED) continue;  // no layout of that width for this tpi
+        if (rc) return rc;
+    }
+    if (settings == 0) return fail(PG_ERR_UNSUPPORTED, "pg_autotune_ex: no compiled layout fits");
+    // 2. the sieve tile's small-prime bound
+    const uint32_t smalls[] = {16384, 65536, 262144};
+    const pg_job_params after_tpi = best.params;
+    for (uint32_t v : smalls) {
+        if (v > p.max_prime && v != smalls[0]) continue;
+        pg_job_params q = after_tpi;
+        if (q.small_limit == v || (q.small_limit == 0 && v == 65536)) continue;  // timed already
+        q.small_limit = v;
+        const int rc = trial(q, 0, m_inc);
+        if (rc == PG_ERR_UNSUPPORTED) continue;
+        if (rc) return rc;
+    }
+    // 3. PRP warps per SM, two windows in flight
+    const uint32_t caps[] = {4, 6, 8, 10, 12};
+    const pg_job_params tuned = best.params;
+    for (uint32_t w : caps) {
+        const int rc = trial(tuned, w, m_inc);
+        if (rc) return rc;
+    }
+    // 4. window size
+    if (flags & PG_TUNE_WINDOW) {
+        const uint32_t cap = best.warps_per_sm;
+        for (uint64_t div : {2ull, 4ull}) {
+            if (m_inc / div < 2) break;
+            const int rc = trial(tuned, cap, (m_inc + div - 1) / div);
+            if (rc) return rc;
+        }
+    }
+    g_last_error.clear();
+    best.settings = settings;
+    *out = best;
+    return PG_OK;
+}
+
 // ============================================================= records
 
 extern "C" double pg_merit(double k_log, uint64_t m, uint64_t gap) { return (double)gap / (k_log + std::log((double)m)); }

@@ -9,7 +9,8 @@
 
 #define PG_LIMB_LIST(X) X(4) X(8) X(12) X(15) X(16) X(20) X(22) X(23) X(24) X(28) X(32) X(36) X(40) X(44) X(48)
 
-#define PG_GROUP_LIST(X) X(8, 3) X(4, 6) X(4, 8) X(4, 10) X(4, 12) X(8, 8) X(8, 12) X(8, 17) X(8, 20)
+#define PG_GROUP_LIST(X) \
+    X(8, 3) X(4, 6) X(4, 8) X(4, 10) X(4, 12) X(8, 8) X(8, 12) X(8, 17) X(8, 20) X(16, 2) X(16, 3) X(16, 9)
 
 // layout codes: L for one thread per number, (T << 16) | L for groups of T lanes
 #define PG_LAYOUT_GROUP(T, L) (((uint32_t)(T) << 16) | (uint32_t)(L))

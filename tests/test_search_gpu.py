@@ -170,7 +170,7 @@ def test_slot_state_errors(pg):
         assert len(job.search(10_000_000, 1_000).ms) == pg.count_m(10_000_000, 1_000, 2310)
 
 
-@pytest.mark.parametrize("tpi", [4, 8])
+@pytest.mark.parametrize("tpi", [4, 8, 16])
 def test_group_layout_search_equals_single_thread(pg, tpi):
     """The lane-group kernels (persistent, plain, confirmation) give the one-thread kernels' gaps."""
     base = pg.Job(503, 2190, 10_000, 20_000_000, max_m_inc=6_000, max_m=2_000_000, rounds=2)
@@ -183,7 +183,7 @@ def test_group_layout_search_equals_single_thread(pg, tpi):
             assert got.stats["confirm_tests"] == want.stats["confirm_tests"]
 
 
-@pytest.mark.parametrize("tpi", [4, 8])
+@pytest.mark.parametrize("tpi", [4, 8, 16])
 def test_group_layout_continuation_past_sl(pg, oracle, tpi):
     """SL far below the gaps on the lane-group kernels: the continuation launches and the trial division
     of extension positions give GMP's gaps."""
@@ -197,11 +197,14 @@ def test_group_layout_continuation_past_sl(pg, oracle, tpi):
     assert res.stats["extended_sides"] > 0
 
 
-def test_P3001_against_gmp(pg):
-    """P=3001, d=2190, X in [-40000, 40000], primes <= 1e10: 4 248-bit operands on 136-word lane groups."""
+@pytest.mark.parametrize("tpi,limbs", [(0, 136), (16, 144)])
+def test_P3001_against_gmp(pg, tpi, limbs):
+    """P=3001, d=2190, X in [-40000, 40000], primes <= 1e10: 4 248-bit operands on lane groups of 8 x 17
+    words (the automatic layout) and 16 x 9 words."""
     g = golden("gaps_P3001_d2190.json")
-    with pg.Job(g["P"], g["d"], g["sl"], g["max_prime"], max_m_inc=64, max_m=g["m_start"] + g["m_inc"]) as job:
-        assert job.info["limbs"] == 136 and job.info["tpi"] == 8
+    with pg.Job(g["P"], g["d"], g["sl"], g["max_prime"], max_m_inc=64, max_m=g["m_start"] + g["m_inc"],
+                tpi=tpi) as job:
+        assert job.info["limbs"] == limbs and job.info["tpi"] == (tpi or 8)
         for m, a, b in zip(g["ms"], g["prev_gap"], g["next_gap"]):
             res = job.search(m, 1)
             assert list(res.ms) == [m]
@@ -232,6 +235,24 @@ def test_autotune_picks_a_valid_faster_setting(pg, tmp_path):
     with pg.Job(337, 2310, 2_000, 5_000_000, max_m_inc=2_000, max_m=2 * 10**7, **knobs) as tuned, \
             pg.Job(337, 2310, 2_000, 5_000_000, max_m_inc=2_000, max_m=2 * 10**7) as plain:
         a, b = tuned.search(10_000_000, 2_000), plain.search(10_000_000, 2_000)
+    assert np.array_equal(a.prev_gap, b.prev_gap) and np.array_equal(a.next_gap, b.next_gap)
+
+
+def test_autotune_ex_sweeps_the_knobs(pg, tmp_path):
+    """pg_autotune_ex times threads per number (1, 4, 8, 16 and automatic), the sieve tile bound, the PRP
+    warps per SM and the window size with two windows in flight; the chosen setting is one of those, at least
+    as fast as the first one timed, gives the same gaps, and is served from the cache the second time."""
+    cache = tmp_path / "tune.json"
+    res = pg.autotune_ex(503, 2190, 2_000, 20_000_000, 1_000_000, 6_000, windows=True, reps=2, cache=cache)
+    assert res["settings"] == 5 + 2 + 5 + 2
+    assert res["knobs"]["tpi"] in (0, 1, 4, 8, 16) and res["knobs"]["small_limit"] in (0, 16384, 65536, 262144)
+    assert res["warps_per_sm"] in (0, 4, 6, 8, 10, 12) and res["window_m"] in (6_000, 3_000, 1_500)
+    assert res["m_per_sec"] >= res["first_m_per_sec"] > 0
+    assert pg.autotune_ex(503, 2190, 2_000, 20_000_000, 1_000_000, 6_000, windows=True, reps=2, cache=cache) == res
+    knobs = {k: v for k, v in res["knobs"].items() if k in ("small_limit", "tpi")}
+    with pg.Job(503, 2190, 2_000, 20_000_000, max_m_inc=6_000, max_m=2_000_000, **knobs) as tuned, \
+            pg.Job(503, 2190, 2_000, 20_000_000, max_m_inc=6_000, max_m=2_000_000) as plain:
+        a, b = tuned.search(1_000_000, 6_000), plain.search(1_000_000, 6_000)
     assert np.array_equal(a.prev_gap, b.prev_gap) and np.array_equal(a.next_gap, b.next_gap)
 
 
