@@ -603,6 +603,7 @@ static int run_sieve(Slot &s, const WinPart &w, bool compact) {
     la.p = T.d_lp;
     la.cinv = T.d_lcinv;
     la.c = T.d_lc;
+    la.wheel = j->d_wheel;
     const uint64_t split = large_split(j, w.nodd);
     PG_CUDA(launch_sieve_large(la, T.wide, split, s.st));
     s.sst.kernel_launches += (split > 0) + (split < T.np);

@@ -116,6 +116,7 @@ struct LargeArgs {
     const void *p;      // uint32 or uint64 primes
     const void *cinv;   // K^-1 mod p, same type
     const void *c;      // K mod p, same type
+    const uint32_t *wheel;  // [words] positions composite in every row (Y = 0, q | Y for q | K)
 };
 
 // --- launchers (pg_kernels.cu); all enqueue on `st` and return cudaError_t

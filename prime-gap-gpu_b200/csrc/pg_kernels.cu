@@ -286,6 +286,15 @@ __device__ __forceinline__ void mark_hit(const LargeArgs &a, uint64_t j, uint32_
     if (r >= 0) atomicOr(&a.bitmaps[(size_t)r * a.words + (idx >> 5)], 1u << (idx & 31));
 }
 
+// The same, skipping positions the K-prime wheel already marks in every row
+// (about two thirds of them at P = 503: Y = 0 and every Y with a factor
+// q | K); the small-prime kernel ORs the wheel into each row, so the rows
+// come out the same with a third of the atomics and rank loads.
+__device__ __forceinline__ void mark_hit(const LargeArgs &a, const uint32_t *s_wheel, uint64_t j, uint32_t idx) {
+    if ((s_wheel[idx >> 5] >> (idx & 31)) & 1u) return;
+    mark_hit(a, j, idx);
+}
+
 // One thread per prime p.  For the odd m = m0 + 2j of the window,
 // p | m*K + 2Y  <=>  j = -Y*K^-1 - m0/2 (mod p), so the residue j(Y) drops
 // by K^-1 each time Y grows by one; every j(Y) inside the window is a hit.
@@ -442,7 +451,7 @@ struct Mod40 {
 // u >= beta, else u + alpha - beta (step a + b).  Otherwise each next hit is
 // one more search.
 template <typename U, typename Mod>
-__device__ __forceinline__ void sieve_prime(const LargeArgs &a, const Mod &md, U c, U ci) {
+__device__ __forceinline__ void sieve_prime(const LargeArgs &a, const uint32_t *s_wheel, const Mod &md, U c, U ci) {
     const U p = md.p;
     const U W = (U)(2u * a.sly);
     const U c2 = (c & 1) ? (U)((c + (uint64_t)p) >> 1) : c >> 1;  // K/2 mod p
@@ -455,7 +464,7 @@ __device__ __forceinline__ void sieve_prime(const LargeArgs &a, const Mod &md, U
         const U u = modsearch_value<U>(A, B, p, W);
         j += md.mul(md.sub(u, B), Ainv);
         if (j >= a.nodd) return;
-        mark_hit(a, j, (uint32_t)u);
+        mark_hit(a, s_wheel, j, (uint32_t)u);
         if ((a.nodd - j - 1) * (uint64_t)(W + 1) >= 2ull * p) {  // two or more further hits expected: walk
             const U alpha = modsearch_value<U>(A, A, p, W);
             const uint64_t sa = 1 + (uint64_t)md.mul(md.sub(alpha, A), Ainv);
@@ -476,7 +485,7 @@ __device__ __forceinline__ void sieve_prime(const LargeArgs &a, const Mod &md, U
                     v = v + alpha - beta;
                 }
                 if (j >= a.nodd) return;
-                mark_hit(a, j, (uint32_t)v);
+                mark_hit(a, s_wheel, j, (uint32_t)v);
             }
         }
         B = u + A >= p ? u + A - p : u + A;  // residue of j + 1
@@ -484,19 +493,23 @@ __device__ __forceinline__ void sieve_prime(const LargeArgs &a, const Mod &md, U
     }
 }
 
-// One thread per prime of [first, first + count).
+// One thread per prime of [first, first + count); the block keeps the wheel
+// row in shared memory.
 template <typename T>
 __global__ void __launch_bounds__(256) k_sieve_large_search(const __grid_constant__ LargeArgs a, uint64_t first,
                                                             uint64_t count) {
+    extern __shared__ uint32_t s_wheel[];
+    for (uint32_t w = threadIdx.x; w < a.words; w += blockDim.x) s_wheel[w] = a.wheel[w];
+    __syncthreads();
     const uint64_t i = first + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= first + count) return;
     const uint64_t p = ((const T *)a.p)[i];
     const uint64_t c = ((const T *)a.c)[i];
     const uint64_t ci = ((const T *)a.cinv)[i];
     if (p < (1ull << 32))
-        sieve_prime<uint32_t, Mod32>(a, Mod32((uint32_t)p), (uint32_t)c, (uint32_t)ci);
+        sieve_prime<uint32_t, Mod32>(a, s_wheel, Mod32((uint32_t)p), (uint32_t)c, (uint32_t)ci);
     else
-        sieve_prime<uint64_t, Mod40>(a, Mod40(p), c, ci);
+        sieve_prime<uint64_t, Mod40>(a, s_wheel, Mod40(p), c, ci);
 }
 
 cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, cudaStream_t st) {
@@ -517,10 +530,11 @@ cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, cu
     if (split < a.np) {  // the rest: modular search for each hit
         const uint64_t count = a.np - split;
         const uint64_t blocks = (count + threads - 1) / threads;
+        const size_t smem = (size_t)a.words * sizeof(uint32_t);
         if (wide)
-            k_sieve_large_search<uint64_t><<<(unsigned)blocks, threads, 0, st>>>(a, split, count);
+            k_sieve_large_search<uint64_t><<<(unsigned)blocks, threads, smem, st>>>(a, split, count);
         else
-            k_sieve_large_search<uint32_t><<<(unsigned)blocks, threads, 0, st>>>(a, split, count);
+            k_sieve_large_search<uint32_t><<<(unsigned)blocks, threads, smem, st>>>(a, split, count);
     }
     return cudaGetLastError();
 }
