@@ -288,7 +288,7 @@ EXTRA = {  # the other workloads, each window searched alone on one GPU
                  min_merit=24.0, windows=3),
     # a slice of the P=3001 window (its first 600 m): 4 248-bit operands, plain-form A/B on the same m
     "P3001_slice": dict(p=3001, d=2190, m_start=1, m_inc=600, sl=40_000, max_prime=10_000_000_000,
-                        min_merit=25.0, windows=2, plain=True),
+                        min_merit=25.0, windows=2, plain=True, plain_windows=1),
 }
 
 
@@ -308,7 +308,8 @@ def run_config(pg, ctx, w: dict) -> dict:
                "sieve_ms": statistics.median(x["sieve_ms"] for x in st), "limbs": job.info["limbs"],
                "tpi": job.info["tpi"], "windows_timed": len(st)}
         if w.get("plain"):
-            pst = [job.search(w["m_start"], w["m_inc"], pg.PG_SEARCH_PLAIN).stats for _ in range(w["windows"])]
+            pst = [job.search(w["m_start"], w["m_inc"], pg.PG_SEARCH_PLAIN).stats
+                   for _ in range(w.get("plain_windows", w["windows"]))]
             pms = statistics.median(x["total_ms"] for x in pst)
             out["plain_ms_per_window"] = pms
             out["plain_m_per_sec"] = n / (pms / 1e3)
@@ -326,9 +327,22 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
     W = WORKLOAD
     m_start, m_inc = rank_window(rank, world, args.m_inc)
     ctx = pg.Context(local_rank)
+    # autotune (pg_autotune_ex) on this rank's window: threads per number, sieve tile bound, PRP warps per SM
+    tune = None
+    knobs = {}
+    if not args.no_tune:
+        t0 = time.perf_counter()
+        tune = pg.autotune_ex(W["p"], W["d"], W["sl"], W["max_prime"], m_start, m_inc, ctx=ctx, reps=2,
+                              confirm_merit=W["min_merit"])
+        tune["seconds"] = time.perf_counter() - t0
+        knobs = {k: tune["knobs"][k] for k in ("small_limit", "tpi")}
+        if args.warps_per_sm is None:
+            args.warps_per_sm = tune["warps_per_sm"]
+    if args.warps_per_sm is None:
+        args.warps_per_sm = 6
     t0 = time.perf_counter()
     job = pg.Job(W["p"], W["d"], W["sl"], W["max_prime"], max_m_inc=m_inc, max_m=max(RANK_STARTS) + m_inc,
-                 rounds=1, confirm_merit=W["min_merit"], ctx=ctx)
+                 rounds=1, confirm_merit=W["min_merit"], ctx=ctx, **knobs)
     setup_s = time.perf_counter() - t0
     imad_peak = ctx.imad_peak()
     dev = torch.device("cuda", local_rank)
@@ -451,17 +465,19 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
         "warmup": args.warmup, "ms_per_step": agg["dev_s"] * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "config": {"workload": workload_name(RANK_STARTS[0], m_inc),
-                   "form": f"persistent, {pg.PG_SEARCH_SLOTS} windows in flight"
+                   "form": ("autotuned " if tune else "") + f"persistent, {pg.PG_SEARCH_SLOTS} windows in flight"
                            + (f", {args.warps_per_sm} PRP warps per SM per window" if args.warps_per_sm else "")
                            + (f", draining to {args.drain} lanes per unresolved side" if args.drain else "")
                            + ", records confirmed with 16 bases",
                    "m_per_gpu_per_step": m_count, "sl": W["sl"], "max_prime": W["max_prime"],
-                   "limbs": limbs, "tpi": job.info["tpi"], "parallelism": f"weak: {world} disjoint m-windows",
+                   "limbs": limbs, "tpi": job.info["tpi"], "small_limit": job.params.small_limit or 65536,
+                   "warps_per_sm": args.warps_per_sm, "parallelism": f"weak: {world} disjoint m-windows",
                    "l2": "inputs larger than L2 (1.18 GB prime tables read every step)"},
         "prp_tests_per_sec": agg["prp_tests_per_sec"],
         "ms_per_step_one_window_alone": max(r["sync_ms"] for r in allr),
         "setup_seconds": setup_s,
         "bit_exact_vs_gmp_sample": exact,
+        "autotune": tune,
         "roofline": roof,
         "sieve": sieve,
         "e2e": {"value": agg["e2e_value"], "unit": "m/s",
@@ -633,9 +649,12 @@ def main(argv=None) -> int:
                          "unresolved side (PG_SUBMIT_DRAIN; 0 = off)")
     ap.add_argument("--warps-per-sm", type=int, default=None, metavar="W",
                     help="cap each launch's PRP kernel at W resident warps per SM so the two launches "
-                         "in flight run side by side (0 = as many as fit; default 6 for the window "
-                         "benchmark, measured best at 22 words, and 0 for --serve, whose launches are "
+                         "in flight run side by side (0 = as many as fit; default: the autotuner's choice for "
+                         "the window benchmark, 6 with --no-tune, and 0 for --serve, whose launches are "
                          "large enough that the cap costs more than it saves)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the autotuner (default knobs: automatic threads per number, 65536 sieve tile "
+                         "bound, 6 warps per SM)")
     ap.add_argument("--m-inc", type=int, default=WORKLOAD["m_inc"],
                     help="m per window (default 200000; smaller windows are for profiling only)")
     ap.add_argument("--serve", action="store_true",
@@ -647,8 +666,8 @@ def main(argv=None) -> int:
     ap.add_argument("--serve-rate", type=float, default=0.0,
                     help="arrival rate in requests/s for the latency run (0 = 70%% of the measured capacity)")
     args = ap.parse_args(argv)
-    if args.warps_per_sm is None:
-        args.warps_per_sm = 0 if args.serve else 6
+    if args.warps_per_sm is None and args.serve:
+        args.warps_per_sm = 0
     if args.serve:
         print(json.dumps(run_serve(args)), flush=True)
         return 0

@@ -127,6 +127,11 @@ typedef struct {
 #define PG_JOB_LARGE_SEARCH 0x2u   /* modular search for the next hit */
 #define PG_JOB_NO_GRAPH     0x4u   /* launch the persistent form's kernels one by one
                                       instead of as one CUDA graph per window */
+#define PG_JOB_COMPACT_WALK 0x8u   /* keep the large-prime sieve's walk steps (8 B per prime below
+                                      2^32, computed at job creation: 0.8 GB at 2e9) only for the
+                                      primes expecting >= 64 hits per window; the others find each
+                                      hit after the first by another modular search.  For short-lived
+                                      jobs (the server sets it for its jobs) */
 
 typedef struct {
     uint32_t k_bits;          /* bits of K */

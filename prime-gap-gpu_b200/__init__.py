@@ -43,6 +43,7 @@ PG_MAX_WORDS = 160
 PG_JOB_LARGE_STEP = 0x1
 PG_JOB_LARGE_SEARCH = 0x2
 PG_JOB_NO_GRAPH = 0x4
+PG_JOB_COMPACT_WALK = 0x8
 
 # every symbol include/primegap.h declares
 EXPORTS = (

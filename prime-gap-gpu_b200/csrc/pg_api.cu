@@ -586,6 +586,41 @@ static uint64_t large_split(const pg_job *j, uint64_t nodd) {
     return std::max(min_split, table_index_at(T, (double)nodd * (2.0 * j->sly + 1) / hits));
 }
 
+// Bands of the segmented large-prime kernel for a window of nodd odd m: the
+// primes with walk steps from max(split, walk_first) up to those expecting
+// about SEG_HITS hits in the window, table segment by table segment (primes
+// of one segment lie within 2^19 of each other), each cut into the power of
+// two of segments that leaves about SEG_HITS expected hits per (prime,
+// segment) item at the segment's smallest prime; neighbouring segments with
+// the same count share a launch.  Returns the first prime index left to the
+// one-thread-per-prime kernel.
+static uint64_t seg_bands(const pg_job *j, uint64_t split, uint64_t nodd, SegBand *bands, int *nb) {
+    *nb = 0;
+    const pg::Tables &T = *j->T;
+    const double width = 2.0 * j->sly + 1;
+    const uint64_t lo = std::max(split, j->walk_first);
+    const uint64_t hi = std::min(j->walk_first + j->walk_count, table_index_at(T, (double)nodd * width / SEG_HITS));
+    if (!j->walk_count || lo >= hi) return split;
+    const size_t nseg_tab = T.seg_off.size();
+    for (size_t s = 0; s < nseg_tab; s++) {
+        const uint64_t a = std::max<uint64_t>(lo, T.seg_off[s]);
+        const uint64_t b = std::min<uint64_t>(hi, s + 1 < nseg_tab ? T.seg_off[s + 1] : T.np);
+        if (a >= b) continue;
+        const double pmin = std::max((double)T.seg_v0 + (double)s * (double)T.seg_span, (double)T.q1 + 1);
+        const double hits = (double)nodd * width / pmin;
+        uint32_t nseg = 1;
+        while (nseg < 32768 && 2.0 * nseg * SEG_HITS <= hits) nseg *= 2;
+        const uint32_t seg_len = (uint32_t)((nodd + nseg - 1) / nseg);
+        SegBand *last = *nb ? &bands[*nb - 1] : nullptr;
+        if (last && last->first + last->count == a && (last->nseg == nseg || *nb == MAX_SEG_BANDS)) {
+            last->count = b - last->first;  // extends the band (a full list keeps its segment count)
+            continue;
+        }
+        bands[(*nb)++] = SegBand{a, b - a, nseg, seg_len};
+    }
+    return hi;
+}
+
 // sieve of one window of the slot into its rows of lists (compact) or into
 // the bitmap rows (the slot's first window only)
 static int run_sieve(Slot &s, const WinPart &w, bool compact) {
@@ -604,9 +639,15 @@ static int run_sieve(Slot &s, const WinPart &w, bool compact) {
     la.cinv = T.d_lcinv;
     la.c = T.d_lc;
     la.wheel = j->d_wheel;
+    la.walk = j->d_walk;
+    la.walk_first = j->walk_first;
+    la.walk_end = j->walk_first + j->walk_count;
     const uint64_t split = large_split(j, w.nodd);
-    PG_CUDA(launch_sieve_large(la, T.wide, split, s.st));
-    s.sst.kernel_launches += (split > 0) + (split < T.np);
+    SegBand bands[MAX_SEG_BANDS];
+    int nb = 0;
+    const uint64_t search_first = seg_bands(j, split, w.nodd, bands, &nb);
+    PG_CUDA(launch_sieve_large(la, T.wide, split, bands, nb, search_first, s.st));
+    s.sst.kernel_launches += (split > 0) + nb + (search_first < T.np);
     SieveArgs sa{};
     sa.sly = j->sly;
     sa.words = j->W;
@@ -856,6 +897,7 @@ static void job_free(pg_job *j) {
     cudaStreamSynchronize(j->ctx->stream);
     for (auto &s : j->slot) slot_free(s);
     cudaFree(j->d_wheel);
+    cudaFree(j->d_walk);
     delete j;  // drops this job's reference to the shared tables
 }
 
@@ -914,6 +956,26 @@ static int job_build(pg_job *j) {
     for (uint64_t r = 1; r <= p.d; r++) phi += gcd64(r, p.d) == 1;
     j->nm_cap = std::min<uint64_t>(j->nodd_cap, (mi / p.d + 1) * phi);
     if (2 * j->nm_cap >= 0xffffffffull) return fail(PG_ERR_UNSUPPORTED, "max_m_inc too large");
+    // ---- walk steps of the large primes below 2^32 for this job's window width
+    // (with PG_JOB_COMPACT_WALK only of those expecting >= SEG_HITS hits in the
+    // largest window, which the segmented kernel needs)
+    if (T.np && !(p.flags & PG_JOB_LARGE_STEP)) {
+        const uint64_t first = table_index_at(T, 2.0 * j->sly + 2);
+        double pmax = (p.flags & PG_JOB_COMPACT_WALK) ? (double)j->nodd_cap * (2.0 * j->sly + 1) / SEG_HITS
+                                                      : 4294967296.0;
+        // table_index_at keeps the whole segment holding pmax: with primes above
+        // 2^32 in the table, stop a segment early so every kept prime is below 2^32
+        if (T.wide) pmax = std::min(pmax, 4294967296.0 - (double)T.seg_span);
+        const uint64_t end = table_index_at(T, pmax);
+        if (end > first) {
+            j->walk_first = first;
+            j->walk_count = end - first;
+            if ((rc = dalloc(j->own_bytes, &j->d_walk, j->walk_count))) return rc;
+            PG_CUDA(launch_walk_consts(T.d_lp, T.d_lc, T.d_lcinv, T.wide, first, j->walk_count, 2 * j->sly,
+                                       j->d_walk, j->ctx->stream));
+            PG_CUDA(cudaStreamSynchronize(j->ctx->stream));
+        }
+    }
     return PG_OK;
 }
 

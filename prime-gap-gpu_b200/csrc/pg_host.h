@@ -157,6 +157,10 @@ struct pg_ctx {
 
 struct pg_job {
     pg_ctx *ctx = nullptr;
+    // walk constants of the many-hit primes [walk_first, walk_first + walk_count)
+    // of the table for this job's window width (segmented large-prime sieve)
+    pg::WalkC *d_walk = nullptr;
+    uint64_t walk_first = 0, walk_count = 0;
     pg_job_params prm{};
     std::shared_ptr<pg::Tables> T;
     uint32_t L = 0, sly = 0, W = 0, cap = 0;

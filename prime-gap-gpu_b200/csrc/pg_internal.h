@@ -105,6 +105,8 @@ struct SieveArgs {
     unsigned long long *survivors;
 };
 
+struct WalkC;
+
 struct LargeArgs {
     uint32_t sly;
     uint32_t words;
@@ -117,7 +119,29 @@ struct LargeArgs {
     const void *cinv;   // K^-1 mod p, same type
     const void *c;      // K mod p, same type
     const uint32_t *wheel;  // [words] positions composite in every row (Y = 0, q | Y for q | K)
+    const struct WalkC *walk;  // walk steps of the primes [walk_first, walk_end), NULL = none
+    uint64_t walk_first, walk_end;
 };
+
+// The three-distance walk of one prime below 2^32: the step counts sa (the
+// first step whose shift A*sa mod p = alpha lands in [0, W]) and sb (the
+// first whose shift lands in [p - W, p), i.e. -beta); alpha = A*sa mod p and
+// beta = p - A*sb mod p follow with two modular products.  They depend on p,
+// K mod p and the window width W only, so a job computes them once.
+struct WalkC {
+    uint32_t sa, sb;
+};
+
+// Primes of the large-prime table processed by the segmented kernel in one
+// launch: [first, first + count), each split into nseg segments of seg_len
+// odd m (thread = prime x segment).
+struct SegBand {
+    uint64_t first, count;
+    uint32_t nseg, seg_len;
+};
+constexpr int MAX_SEG_BANDS = 24;
+// expected hits per (prime, segment) item the bands aim at
+constexpr uint32_t SEG_HITS = 64;
 
 // --- launchers (pg_kernels.cu); all enqueue on `st` and return cudaError_t
 cudaError_t launch_prime_count(uint64_t v_first, uint64_t limit, const uint32_t *base, uint32_t nbase,
@@ -131,7 +155,14 @@ cudaError_t launch_prime_tables(const uint32_t *K, uint32_t kwords, uint64_t np,
 cudaError_t launch_prime_reorder(uint64_t np, uint32_t nseg, const uint64_t *seg_off, const void *p, const void *c,
                                  const void *ci, void *op, void *oc, void *oci, uint8_t *depth, bool wide,
                                  cudaStream_t st);
-cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, cudaStream_t st);
+// Large-prime sieve of one window: primes [0, split) step every Y; the bands
+// run the segmented walk (the walk steps of a.walk); primes [search_first,
+// np) one thread each (modular search for the first hit, then the walk).
+cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, const SegBand *bands, int nbands,
+                               uint64_t search_first, cudaStream_t st);
+// walk constants of the primes [first, first + count) (all < 2^32) for width W
+cudaError_t launch_walk_consts(const void *p, const void *c, const void *ci, bool wide, uint64_t first,
+                               uint64_t count, uint32_t W, WalkC *out, cudaStream_t st);
 cudaError_t launch_sieve_small(const SieveArgs &a, bool compact, cudaStream_t st);
 cudaError_t launch_prp_batch(uint32_t L, const uint32_t *cand, uint32_t words, uint32_t n, uint32_t rounds,
                              int32_t *out, cudaStream_t st);

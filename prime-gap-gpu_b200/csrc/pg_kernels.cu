@@ -450,8 +450,13 @@ struct Mod40 {
 // after u is u + alpha (step a) if that is <= W, else u - beta (step b) if
 // u >= beta, else u + alpha - beta (step a + b).  Otherwise each next hit is
 // one more search.
+//
+// With the job's walk steps (wk != NULL: sa, sb precomputed, alpha and beta
+// two modular products away) every hit after the first is one walk step,
+// whatever the number of hits.
 template <typename U, typename Mod>
-__device__ __forceinline__ void sieve_prime(const LargeArgs &a, const uint32_t *s_wheel, const Mod &md, U c, U ci) {
+__device__ __forceinline__ void sieve_prime(const LargeArgs &a, const uint32_t *s_wheel, const Mod &md, U c, U ci,
+                                            const WalkC *wk) {
     const U p = md.p;
     const U W = (U)(2u * a.sly);
     const U c2 = (c & 1) ? (U)((c + (uint64_t)p) >> 1) : c >> 1;  // K/2 mod p
@@ -465,13 +470,22 @@ __device__ __forceinline__ void sieve_prime(const LargeArgs &a, const uint32_t *
         j += md.mul(md.sub(u, B), Ainv);
         if (j >= a.nodd) return;
         mark_hit(a, s_wheel, j, (uint32_t)u);
-        if ((a.nodd - j - 1) * (uint64_t)(W + 1) >= 2ull * p) {  // two or more further hits expected: walk
-            const U alpha = modsearch_value<U>(A, A, p, W);
-            const uint64_t sa = 1 + (uint64_t)md.mul(md.sub(alpha, A), Ainv);
-            const U aw = A + W >= p ? A + W - p : A + W;
-            const U ub = modsearch_value<U>(A, aw, p, W - 1);
-            const U beta = W - ub;
-            const uint64_t sb = 1 + (uint64_t)md.mul(md.sub(ub, aw), Ainv);
+        if (wk || (a.nodd - j - 1) * (uint64_t)(W + 1) >= 2ull * p) {  // steps known, or 2+ hits expected: walk
+            U alpha, beta;
+            uint64_t sa, sb;
+            if (wk) {
+                sa = wk->sa;
+                sb = wk->sb;
+                alpha = md.mul(A, (U)sa);
+                beta = p - md.mul(A, (U)sb);
+            } else {
+                alpha = modsearch_value<U>(A, A, p, W);
+                sa = 1 + (uint64_t)md.mul(md.sub(alpha, A), Ainv);
+                const U aw = A + W >= p ? A + W - p : A + W;
+                const U ub = modsearch_value<U>(A, aw, p, W - 1);
+                beta = W - ub;
+                sb = 1 + (uint64_t)md.mul(md.sub(ub, aw), Ainv);
+            }
             U v = u;
             while (true) {
                 if (v + alpha <= W) {
@@ -506,16 +520,113 @@ __global__ void __launch_bounds__(256) k_sieve_large_search(const __grid_constan
     const uint64_t p = ((const T *)a.p)[i];
     const uint64_t c = ((const T *)a.c)[i];
     const uint64_t ci = ((const T *)a.cinv)[i];
+    const bool walk = a.walk && i >= a.walk_first && i < a.walk_end;  // walk steps are kept below 2^32 only
+    WalkC wk;
+    if (walk) wk = a.walk[i - a.walk_first];
     if (p < (1ull << 32))
-        sieve_prime<uint32_t, Mod32>(a, s_wheel, Mod32((uint32_t)p), (uint32_t)c, (uint32_t)ci);
+        sieve_prime<uint32_t, Mod32>(a, s_wheel, Mod32((uint32_t)p), (uint32_t)c, (uint32_t)ci, walk ? &wk : nullptr);
     else
-        sieve_prime<uint64_t, Mod40>(a, s_wheel, Mod40(p), c, ci);
+        sieve_prime<uint64_t, Mod40>(a, s_wheel, Mod40(p), c, ci, nullptr);
 }
 
-cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, cudaStream_t st) {
+// Walk constants (alpha, sa, beta, sb of sieve_prime) of the primes
+// [first, first + count), all below 2^32, for the window width W.
+template <typename T>
+__global__ void __launch_bounds__(256) k_walk_consts(const T *pt, const T *ct, const T *cit, uint64_t first,
+                                                     uint64_t count, uint32_t W, WalkC *out) {
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const uint32_t p = (uint32_t)pt[first + k], c = (uint32_t)ct[first + k];
+    const Mod32 md(p);
+    const uint32_t A = p - c, Ainv = p - (uint32_t)cit[first + k];  // -K and (-K)^-1
+    const uint32_t alpha = modsearch_value<uint32_t>(A, A, p, W);
+    const uint32_t aw = A + W >= p ? A + W - p : A + W;
+    const uint32_t ub = modsearch_value<uint32_t>(A, aw, p, W - 1);
+    WalkC w;
+    w.sa = 1 + md.mul(md.sub(alpha, A), Ainv);
+    w.sb = 1 + md.mul(md.sub(ub, aw), Ainv);
+    out[k] = w;
+}
+
+cudaError_t launch_walk_consts(const void *p, const void *c, const void *ci, bool wide, uint64_t first,
+                               uint64_t count, uint32_t W, WalkC *out, cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
+    const uint64_t blocks = (count + 255) / 256;
+    if (wide)
+        k_walk_consts<uint64_t><<<(unsigned)blocks, 256, 0, st>>>((const uint64_t *)p, (const uint64_t *)c,
+                                                                   (const uint64_t *)ci, first, count, W, out);
+    else
+        k_walk_consts<uint32_t><<<(unsigned)blocks, 256, 0, st>>>((const uint32_t *)p, (const uint32_t *)c,
+                                                                   (const uint32_t *)ci, first, count, W, out);
+    return cudaGetLastError();
+}
+
+// Segmented sieve of the many-hit primes (below 2^32): thread (prime i,
+// segment blockIdx.y) covers the odd m j in [j0, j1) of its segment.  The
+// first hit at j >= j0 comes from one modular search from the residue at j0,
+// (A*j0 + B) mod p; every later hit of the segment from the prime's walk
+// constants.  A prime expecting thousands of hits per window is thus spread
+// over many threads of similar work instead of one long serial walk.
+template <typename T>
+__global__ void __launch_bounds__(256) k_sieve_large_seg(const __grid_constant__ LargeArgs a, uint64_t first,
+                                                         uint64_t count, uint32_t seg_len) {
+    extern __shared__ uint32_t s_wheel[];
+    for (uint32_t w = threadIdx.x; w < a.words; w += blockDim.x) s_wheel[w] = a.wheel[w];
+    __syncthreads();
+    const uint64_t i = first + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t j0 = (uint64_t)blockIdx.y * seg_len;
+    if (i >= first + count || j0 >= a.nodd) return;
+    const uint64_t j1 = min(a.nodd, j0 + seg_len);
+    const uint32_t p = (uint32_t)((const T *)a.p)[i];
+    const uint32_t c = (uint32_t)((const T *)a.c)[i];
+    const uint32_t ci = (uint32_t)((const T *)a.cinv)[i];
+    const WalkC wk = a.walk[i - a.walk_first];
+    const Mod32 md(p);
+    const uint32_t W = 2u * a.sly;
+    const uint32_t c2 = (c & 1) ? (uint32_t)((c + (uint64_t)p) >> 1) : c >> 1;  // K/2 mod p
+    const uint32_t A = p - c, Ainv = p - ci;
+    const uint32_t alpha = md.mul(A, wk.sa), beta = p - md.mul(A, wk.sb);
+    const uint32_t B0 = md.sub(a.sly % p, md.mul(md.red(a.m0), c2));
+    const uint32_t B = md.red((uint64_t)md.mul(A, md.red(j0)) + B0);  // residue at j0
+    const uint32_t u = modsearch_value<uint32_t>(A, B, p, W);
+    uint64_t j = j0 + md.mul(md.sub(u, B), Ainv);
+    if (j >= j1) return;
+    mark_hit(a, s_wheel, j, u);
+    uint32_t v = u;
+    while (true) {
+        if (v + alpha <= W) {
+            j += wk.sa;
+            v += alpha;
+        } else if (v >= beta) {
+            j += wk.sb;
+            v -= beta;
+        } else {
+            j += (uint64_t)wk.sa + wk.sb;
+            v = v + alpha - beta;
+        }
+        if (j >= j1) return;
+        mark_hit(a, s_wheel, j, v);
+    }
+}
+
+cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, const SegBand *bands, int nbands,
+                               uint64_t search_first, cudaStream_t st) {
     if (a.np == 0) return cudaSuccess;
     const uint32_t threads = 256;
+    const size_t smem = (size_t)a.words * sizeof(uint32_t);
     if (split > a.np) split = a.np;
+    for (int b = 0; b < nbands; b++) {
+        const SegBand &bd = bands[b];
+        if (bd.count == 0) continue;
+        const dim3 grid((unsigned)((bd.count + threads - 1) / threads), bd.nseg);
+        if (wide)
+            k_sieve_large_seg<uint64_t><<<grid, threads, smem, st>>>(a, bd.first, bd.count, bd.seg_len);
+        else
+            k_sieve_large_seg<uint32_t><<<grid, threads, smem, st>>>(a, bd.first, bd.count, bd.seg_len);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (search_first < split) search_first = split;
     if (split > 0) {  // primes with many hits per window: step every Y
         LargeArgs s = a;
         s.np = split;
@@ -527,14 +638,13 @@ cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, cu
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
-    if (split < a.np) {  // the rest: modular search for each hit
-        const uint64_t count = a.np - split;
+    if (search_first < a.np) {  // the rest: modular search for each hit
+        const uint64_t count = a.np - search_first;
         const uint64_t blocks = (count + threads - 1) / threads;
-        const size_t smem = (size_t)a.words * sizeof(uint32_t);
         if (wide)
-            k_sieve_large_search<uint64_t><<<(unsigned)blocks, threads, smem, st>>>(a, split, count);
+            k_sieve_large_search<uint64_t><<<(unsigned)blocks, threads, smem, st>>>(a, search_first, count);
         else
-            k_sieve_large_search<uint32_t><<<(unsigned)blocks, threads, smem, st>>>(a, split, count);
+            k_sieve_large_search<uint32_t><<<(unsigned)blocks, threads, smem, st>>>(a, search_first, count);
     }
     return cudaGetLastError();
 }

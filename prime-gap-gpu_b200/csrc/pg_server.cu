@@ -198,7 +198,7 @@ struct pg_server {
         p.small_limit = prm.small_limit;
         p.ext_window = prm.ext_window;
         p.tpi = prm.tpi;
-        p.flags = PG_JOB_NO_GRAPH;
+        p.flags = PG_JOB_NO_GRAPH | PG_JOB_COMPACT_WALK;  // jobs come and go with requests
         pg_job *j = nullptr;
         int rc = job_create(ctx, p, &j);
         if (rc) return rc;

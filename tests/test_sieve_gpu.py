@@ -42,7 +42,7 @@ def test_rows_match_oracle(pg, oracle, P, d, sl, limit, m_start, m_inc, small):
     assert np.array_equal(rows, want)
 
 
-@pytest.mark.parametrize("flags", [0, 1, 2])  # automatic split, step every Y, modular search
+@pytest.mark.parametrize("flags", [0, 1, 2, 8])  # automatic split, step every Y, modular search, compact walk table
 @pytest.mark.parametrize("P,d,sl,limit,m_start,m_inc", [
     (503, 2190, 10_000, 30_000_000, 1_000_000, 4_000),
     (337, 2310, 200_000 // 2, 5_000_000, 10_000_000, 1_000),   # sly = 50 000 < small split: two hits per j
@@ -125,3 +125,19 @@ def test_random_sieve_rows(pg, oracle, shape):
         assert np.array_equal(ms, oracle.coprime_ms(m_start, m_inc, d))
         want = oj.sieve_m(ms)
     assert np.array_equal(rows, want)
+
+
+@pytest.mark.parametrize("P,d,sl,limit,small,m_start,m_inc", [
+    (503, 2190, 10_000, 20_000_000, 1_000, 1_000_000, 50_000),   # p from 10 007: 256 segments of 98 odd m
+    (907, 210, 2_000, 8_000_000, 2_000, 1_000_000, 40_000),      # p from 4 001: 64 segments
+    (337, 2310, 64, 3_000_000, 0, 10_000_000, 60_000),           # sl 64: walks of width 65
+])
+def test_segmented_large_prime_rows(pg, oracle, P, d, sl, limit, small, m_start, m_inc):
+    """Primes that expect many hits per window are sieved by (prime, segment of m) threads from walk
+    constants computed once per job; sampled rows of a wide window equal the oracle's, and a second, smaller
+    window on the same job (fewer segments per prime) too."""
+    with _job(pg, P, d, sl, limit, m_start, m_inc, small_limit=small) as job, oracle.Job(P, d, sl, limit) as oj:
+        for start, inc in [(m_start, m_inc), (m_start + 999, m_inc // 7)]:
+            ms, rows = job.sieve_interval(start, inc)
+            sel = np.arange(0, len(ms), 53)
+            assert np.array_equal(rows[sel], oj.sieve_m(ms[sel]))
