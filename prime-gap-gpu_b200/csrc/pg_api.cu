@@ -317,6 +317,10 @@ static int tables_build(pg::Tables &T, const pg_job_params &p, cudaStream_t st) 
         }
     }
     T.nsmall = (uint32_t)sq.size();
+    for (uint32_t q : sq) {
+        T.n32 += q < 32;
+        T.n256 += q < 256;
+    }
     int rc;
     if ((rc = dalloc(T.bytes, &T.d_sq, sq.size())) || (rc = dalloc(T.bytes, &T.d_sr, sr.size())) ||
         (rc = dalloc(T.bytes, &T.d_sbar, sbar.size())) || (rc = dalloc(T.bytes, &T.d_tq, TRIAL_PRIMES)))
@@ -663,6 +667,8 @@ static int run_sieve(Slot &s, const WinPart &w, bool compact) {
     sa.sr = T.d_sr;
     sa.sbar = T.d_sbar;
     sa.nsmall = T.nsmall;
+    sa.n32 = T.n32;
+    sa.n256 = T.n256;
     sa.lists = s.d_lists + (size_t)2 * w.m_off * s.stride;
     sa.counts = s.d_counts + (size_t)2 * w.m_off;
     sa.max_count = &s.d_sc->max_count;

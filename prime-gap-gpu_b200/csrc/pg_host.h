@@ -52,6 +52,7 @@ struct Tables {
     uint32_t *d_sq = nullptr, *d_sr = nullptr;
     uint64_t *d_sbar = nullptr;
     uint32_t nsmall = 0;
+    uint32_t n32 = 0, n256 = 0;  // small primes (ascending) below 32 and below 256
     uint32_t *d_tq = nullptr;   // trial primes 3, 5, 7, ...
     std::vector<uint32_t> tr;   // their residues (-(K mod q)/2) mod q
     void *d_lp = nullptr, *d_lc = nullptr, *d_lcinv = nullptr;

@@ -99,6 +99,7 @@ struct SieveArgs {
     const uint32_t *sr;
     const uint64_t *sbar;
     uint32_t nsmall;
+    uint32_t n32, n256;      // the first n32 small primes are below 32, the first n256 below 256
     uint16_t *lists;
     uint32_t *counts;
     uint32_t *max_count;

@@ -653,18 +653,52 @@ cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, co
 
 constexpr int SMALL_THREADS = 256;
 
+// First marked position of small prime i in the row of m: p | m*K + 2Y
+// <=> Y = (m mod q) * r_q (mod q), position idx = Y + sly.
+__device__ __forceinline__ uint32_t small_first(const SieveArgs &a, uint32_t i, uint64_t m) {
+    const uint32_t q = a.sq[i];
+    const uint64_t bar = a.sbar[i];
+    const uint32_t mq = barrett64(m, q, bar);
+    const uint32_t y0 = barrett64((uint64_t)mq * a.sr[i], q, bar);
+    uint32_t idx = y0 + barrett64(a.sly, q, bar);
+    return idx >= q ? idx - q : idx;
+}
+
 // One block per m.  The row starts as the K-prime wheel OR the large-prime
 // hits, the small primes are struck out in shared memory, then the survivors
-// of each side are compacted, nearest first, into that side's list.
+// of each side are compacted, nearest first, into that side's list.  Primes
+// below 32 (odd d-primes such as 3 and 5 hit a third and a fifth of the row)
+// are laid on whole words by the thread that owns the word, as it loads the
+// row; primes below 256 are marked by all threads of the block, each taking
+// every blockDim-th hit; the rest one prime per thread.  A row's work is thus
+// spread over the block instead of waiting on the thread of q = 3.
 __global__ void __launch_bounds__(SMALL_THREADS) k_sieve_small(const __grid_constant__ SieveArgs a, int compact) {
     extern __shared__ uint32_t bm[];
+    __shared__ uint32_t s_first[64];  // first positions of the primes below 32 (at most 10 of them)
     const uint32_t r = blockIdx.x;
     const uint64_t m = a.ms[r];
     const uint32_t W = a.words, sly = a.sly, nb = 2 * sly + 1;
     uint32_t *grow = a.bitmaps + (size_t)r * W;
-    for (uint32_t w = threadIdx.x; w < W; w += blockDim.x) bm[w] = a.wheel[w] | grow[w];
+    if (threadIdx.x < a.n32) s_first[threadIdx.x] = small_first(a, threadIdx.x, m);
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < a.nsmall; i += blockDim.x) {
+    for (uint32_t w = threadIdx.x; w < W; w += blockDim.x) {
+        uint32_t pm = 0;
+        for (uint32_t i = 0; i < a.n32; i++) {  // bits 32w + b with b = first - 32w (mod q), stride q
+            const uint32_t q = a.sq[i];
+            const uint32_t base = (32u * w) % q;
+            uint32_t b = s_first[i] >= base ? s_first[i] - base : s_first[i] + q - base;
+            for (; b < 32; b += q) pm |= 1u << b;
+        }
+        if (32u * w + 32u > nb) pm &= (1u << (nb - 32u * w)) - 1u;  // no marks past position 2 sly
+        bm[w] = a.wheel[w] | grow[w] | pm;
+    }
+    __syncthreads();
+    for (uint32_t i = a.n32; i < a.n256; i++) {  // all threads stride over the hits of each prime below 256
+        const uint32_t q = a.sq[i];
+        for (uint32_t idx = small_first(a, i, m) + threadIdx.x * q; idx < nb; idx += blockDim.x * q)
+            atomicOr(&bm[idx >> 5], 1u << (idx & 31));
+    }
+    for (uint32_t i = a.n256 + threadIdx.x; i < a.nsmall; i += blockDim.x) {
         const uint32_t q = a.sq[i];
         const uint64_t bar = a.sbar[i];
         const uint32_t mq = barrett64(m, q, bar);
