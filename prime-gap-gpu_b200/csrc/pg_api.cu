@@ -493,7 +493,7 @@ void pg::slot_free(Slot &s) {
     void *ptrs[] = {s.d_ms,   s.d_wid,  s.d_rank, s.d_bitmaps, s.d_lists, s.d_counts, s.d_found, s.d_kstart,
                     s.d_knext, s.d_gaps, s.d_act0, s.d_act1,    s.d_redo,  s.d_conf,   s.d_sc,     s.d_win};
     for (void *p : ptrs) cudaFree(p);
-    void *hptrs[] = {s.h_sc, s.h_ms, s.h_wid, s.h_rank, s.h_gaps, s.h_win};
+    void *hptrs[] = {s.h_sc, s.h_ms, s.h_wid, s.h_rank, s.h_gaps, s.h_win, (void *)s.h_stop};
     for (void *p : hptrs) cudaFreeHost(p);
     for (auto &e : s.ev)
         if (e) cudaEventDestroy(e);
@@ -747,6 +747,12 @@ static int enqueue_windows(Slot &s, int form, uint32_t flags) {
             a.drain_lanes = d ? d : 4;
             a.min_warps = (uint32_t)sms;
         }
+        if (s.d_stop) {
+            *s.h_stop = 0;
+            a.stop = s.d_stop;
+            a.stopped = &s.d_sc->stopped;
+        }
+        s.search = a;
         PG_CUDA(record_ev(s.ev[3], s.st));
         PG_CUDA(launch_search_persistent(s.L, a, s.grid, s.st));
         PG_CUDA(record_ev(s.ev[4], s.st));
@@ -779,6 +785,37 @@ static int enqueue_windows(Slot &s, int form, uint32_t flags) {
     a.act = s.d_act0;
     a.n_act = S;
     a.max_count = nullptr;
+    a.stop = nullptr;  // finalize reads `stopped` only
+    return enqueue_finalize(s, a, S);
+}
+
+int pg::slot_enable_preempt(Slot &s) {
+    if (s.h_stop) return PG_OK;
+    uint32_t *h = nullptr;
+    PG_CUDA(cudaHostAlloc((void **)&h, sizeof(uint32_t), cudaHostAllocMapped));
+    *h = 0;
+    s.h_stop = h;
+    PG_CUDA(cudaHostGetDevicePointer((void **)&s.d_stop, h, 0));
+    return PG_OK;
+}
+
+void pg::slot_preempt(Slot &s) {
+    if (s.h_stop) *s.h_stop = 1;
+}
+
+int pg::slot_resume(Slot &s) {
+    if (!s.d_stop) return fail(PG_ERR_STATE, "slot_resume: the slot has no stop flag");
+    *s.h_stop = 0;
+    const uint32_t S = 2 * s.nm;
+    PG_CUDA(cudaMemsetAsync(&s.d_sc->stopped, 0, 4, s.st));
+    PG_CUDA(launch_search_persistent(s.L, s.search, s.grid, s.st));
+    s.sst.kernel_launches++;
+    s.sst.relaunches++;
+    SearchArgs a = s.search;
+    a.act = s.d_act0;
+    a.n_act = S;
+    a.max_count = nullptr;
+    a.stop = nullptr;
     return enqueue_finalize(s, a, S);
 }
 
@@ -827,6 +864,7 @@ int pg::slot_enqueue(Slot &s, int form, uint32_t flags, bool graph) {
 int pg::slot_finish(Slot &s) {
     PG_CUDA(cudaStreamSynchronize(s.st));
     if (s.nm == 0) return PG_OK;
+    if (s.h_sc->stopped) return SLOT_STOPPED;  // preempted before its queue ran out: slot_resume
     const uint32_t S = 2 * s.nm;
     SearchArgs a = base_args(s);
     uint32_t ext_done = s.ext_window;

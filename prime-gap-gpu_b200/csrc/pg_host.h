@@ -24,6 +24,7 @@
 namespace pg {
 
 constexpr int SLOT_FULL = 1;
+constexpr int SLOT_STOPPED = 2;  // slot_finish: the search was preempted; slot_resume continues it
 
 // records the calling thread's error text and returns code
 int fail(int code, const char *fmt, ...);
@@ -115,6 +116,11 @@ struct Slot {
     uint32_t stride = 0;   // list stride (largest job capacity)
     uint32_t ext_window = 0;
     bool confirm = false;  // a window of the slot confirms the primes of its large gaps
+    // preemption (serving): stop flag in mapped pinned host memory, read by the
+    // persistent search; the search's arguments are kept for the resume
+    volatile uint32_t *h_stop = nullptr;
+    uint32_t *d_stop = nullptr;
+    SearchArgs search{};
     int grid = 0;
     bool busy = false;
     uint64_t ticket = 0;
@@ -138,6 +144,14 @@ int slot_enqueue(Slot &s, int form, uint32_t flags, bool graph);
 // Waits for the queued work, continues unresolved sides past sl, and fills
 // the slot's stats.  Gaps are then in h_gaps (next side 2i, prev side 2i+1).
 int slot_finish(Slot &s);
+// Gives the slot a stop flag: its persistent searches can be preempted.
+int slot_enable_preempt(Slot &s);
+// Raises the stop flag of the slot's running search (host write, no call into
+// the device); its warps leave after the items in hand.
+void slot_preempt(Slot &s);
+// Continues a search whose slot_finish returned SLOT_STOPPED: relaunches the
+// persistent search from its queue head and finalize, on the slot's stream.
+int slot_resume(Slot &s);
 
 int job_create(pg_ctx *c, const pg_job_params &p, pg_job **out);
 

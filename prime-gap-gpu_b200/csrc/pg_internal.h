@@ -66,6 +66,12 @@ struct SearchArgs {
     uint32_t *active_warps;    // warps of this launch still pulling work
     uint32_t drain_lanes;
     uint32_t min_warps;        // never retire below this many warps
+    // preemption (the server's launches): while *stop is nonzero warps take
+    // no new items and leave once their items in hand are tested; a warp that
+    // leaves with items still queued sets *stopped, finalize then writes
+    // nothing, and a relaunch with the same arguments resumes at the queue head
+    const volatile uint32_t *stop;  // NULL = never stop
+    uint32_t *stopped;
 };
 
 // Device scalars of one window slot.
@@ -79,7 +85,7 @@ struct Scalars {
     uint32_t max_count;
     uint32_t unresolved;
     uint32_t active_warps;
-    uint32_t pad;
+    uint32_t stopped;  // the search left items queued (preempted)
 };
 
 // Arguments of the sieve kernels for one window.

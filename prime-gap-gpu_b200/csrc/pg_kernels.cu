@@ -838,6 +838,7 @@ __global__ void k_init_search(uint32_t S, uint32_t *found_k, uint32_t *k_start, 
         sc->n_out = 0;
         sc->unresolved = S;
         sc->active_warps = warps;
+        sc->stopped = 0;
     }
 }
 

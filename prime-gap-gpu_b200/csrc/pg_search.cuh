@@ -81,6 +81,20 @@ __device__ __forceinline__ void build_candidate(const uint32_t *__restrict__ K, 
 
 __device__ __forceinline__ uint32_t load_found(const uint32_t *p) { return *(volatile const uint32_t *)p; }
 
+// Preemption check of a persistent search warp (a.stop set), called by the
+// whole warp: once the flag is raised the warp takes no more items
+// (exhausted); if items are still queued the launch is marked stopped, so
+// finalize skips it and the host resumes it.  Lane 0 reads the flags.
+__device__ __forceinline__ void stop_check(const SearchArgs &a, unsigned long long total, bool &exhausted) {
+    const bool lead = (threadIdx.x & 31) == 0;
+    uint32_t st = 0;
+    if (lead) st = *a.stop;
+    if (__shfl_sync(0xffffffffu, st, 0)) {
+        exhausted = true;
+        if (lead && *(volatile unsigned long long *)a.next_item < total) atomicExch(a.stopped, 1u);
+    }
+}
+
 // Resolves work item (side s, k-th candidate) to its position Y, or returns
 // false when the item needs no test: the side already has a probable prime
 // at a smaller k, the item lies past this launch's extension window, or an
@@ -133,6 +147,7 @@ __global__ void __launch_bounds__(PERSIST_THREADS, PG_PERSIST_MIN_BLOCKS) k_sear
     uint32_t s = 0, k = 0, Y = 0;
     unsigned long long ntests = 0;
     while (true) {
+        if (a.stop && !exhausted) stop_check(a, total, exhausted);
         // Draining: once the unresolved sides are few, extra lanes would only
         // test candidates beyond a prime about to be found; such a warp leaves
         // (with no item in hand) so its SM slot can run other work.  The last
@@ -218,6 +233,7 @@ __global__ void __launch_bounds__(128) k_finalize(const __grid_constant__ Search
                                                   unsigned long long *confirm_tests, uint32_t *k_start_rw) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n_act) return;
+    if (a.stopped && *(volatile const uint32_t *)a.stopped) return;  // preempted: resumed later
     const uint32_t s = a.act[i];
     (void)nsides;
     const uint32_t k = a.found_k[s];

@@ -93,6 +93,7 @@ __global__ void __launch_bounds__(PERSIST_THREADS) k_search_persistent_g(const _
     unsigned long long ntests = 0;
     while (true) {
         __syncwarp();
+        if (a.stop && !exhausted) stop_check(a, total, exhausted);
         if (a.drain_lanes && !exhausted) {
             int retire = 0;
             if (G.lane == 0) {
@@ -183,6 +184,7 @@ __global__ void __launch_bounds__(128) k_finalize_g(const __grid_constant__ Sear
     const Group<T> G;
     const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) / T;
     if (i >= a.n_act) return;
+    if (a.stopped && *(volatile const uint32_t *)a.stopped) return;  // preempted: resumed later
     (void)nsides;
     const uint32_t s = a.act[i];
     const uint32_t k = a.found_k[s];
