@@ -494,7 +494,8 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
     if world == 1 and not args.no_extra:
         line["configs"] = {name: run_config(pg, ctx, w) for name, w in EXTRA.items()}
         ctx.close()
-        line["configs"]["serving"] = run_serve(args, n_jobs=64, compact=True)
+        line["configs"]["serving"] = run_serve(args, n_jobs=64, compact=True, preempt=0)
+        line["configs"]["serving_preempt"] = run_serve(args, n_jobs=64, compact=True, preempt=SERVE_PREEMPT_US)
     else:
         ctx.close()
     if world == 1 and not args.no_cpu:
@@ -534,6 +535,7 @@ def run_reference(args) -> dict:
 # ----------------------------------------------------------- serving
 
 SERVE_SEED = 4
+SERVE_PREEMPT_US = 20_000  # a launch running 20 ms yields to windows that have waited as long
 
 
 def serve_requests(n: int = 256, seed: int = SERVE_SEED, limit: int = 1_000_000_000) -> list[tuple]:
@@ -562,11 +564,12 @@ def serve_requests(n: int = 256, seed: int = SERVE_SEED, limit: int = 1_000_000_
     return out
 
 
-def run_serve(args, n_jobs: int | None = None, compact: bool = False) -> dict:
+def run_serve(args, n_jobs: int | None = None, compact: bool = False, preempt: int | None = None) -> dict:
     """Capacity (all requests queued at once) and latency under Poisson
     arrivals at 70% of that capacity, through pg_server_*.  compact: the
     short run of the default bench line (n_jobs requests, the server's
-    default launch shape)."""
+    default launch shape); preempt: the server's preempt_us (None = the
+    --serve-preempt-us option)."""
     import threading
     import numpy as np
     import __graft_entry__
@@ -577,7 +580,8 @@ def run_serve(args, n_jobs: int | None = None, compact: bool = False) -> dict:
     wps = 0 if compact else args.warps_per_sm
     batch_m = 0 if compact else args.serve_batch_m
     slots = 0 if compact else args.serve_slots
-    with pg.Server(0, max_sl=max_sl, warps_per_sm=wps, batch_m=batch_m, slots=slots) as srv:
+    preempt_us = preempt if preempt is not None else args.serve_preempt_us
+    with pg.Server(0, max_sl=max_sl, warps_per_sm=wps, batch_m=batch_m, slots=slots, preempt_us=preempt_us) as srv:
         # resident tables for every (P, d) first: one small request per class
         warm = [srv.submit(p, d, 1_000, reqs[0][3], 1_000_001, 200) for p, d in classes]
         t = time.perf_counter()
@@ -630,7 +634,9 @@ def run_serve(args, n_jobs: int | None = None, compact: bool = False) -> dict:
         "n_gpus": 1, "data": "synthetic (seeded request mix)",
         "config": {"workload": f"{len(reqs)} requests, P in {{337,503,907}}, d in {{210,2190,2310}}, "
                                "500-20000 m from [1e6,1e9], SL=round(8 ln N), primes <= 1e9",
-                   "seed": SERVE_SEED, "warps_per_sm": wps, "batch_m": batch_m or 65536, "slots": slots or 2},
+                   "seed": SERVE_SEED, "warps_per_sm": wps, "batch_m": batch_m or 65536,
+                   "slots": slots or (3 if preempt_us else 2), "preempt_us": preempt_us},
+        "preemptions": st["preemptions"],
     }
 
 
@@ -663,6 +669,8 @@ def main(argv=None) -> int:
     ap.add_argument("--serve-batch-m", type=int, default=0,
                     help="coprime m per search launch of the server (0 = its default, 65536)")
     ap.add_argument("--serve-slots", type=int, default=0, help="server launch slots (0 = its default, 2)")
+    ap.add_argument("--serve-preempt-us", type=int, default=0,
+                    help="server preemption (pg_server_params.preempt_us; 0 = off)")
     ap.add_argument("--serve-rate", type=float, default=0.0,
                     help="arrival rate in requests/s for the latency run (0 = 70%% of the measured capacity)")
     args = ap.parse_args(argv)

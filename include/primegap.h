@@ -318,8 +318,16 @@ typedef struct {
     uint32_t tpi;          /* as pg_job_params (0 = automatic) */
     uint32_t warps_per_sm; /* cap on each launch's PRP warps per SM (PG_SUBMIT_WARPS_PER_SM), so the
                               launches in flight share the SMs; 0 = as many as fit */
-    uint32_t slots;        /* launches in flight (own stream and buffers each); 0 = 2, at most 8 */
-    uint32_t pad;
+    uint32_t slots;        /* launch slots (own stream and buffers each); 0 = 2 (3 with preemption),
+                              at most 8 */
+    uint32_t preempt_us;   /* preemption of running launches: 0 = off.  Otherwise at most slots - 1
+                              launches run; once windows have waited preempt_us microseconds and a
+                              launch has run as long, that launch's persistent search is told to
+                              stop (its warps leave after the tests in hand), its slot holds the
+                              search's state, the waiting windows run in the free slot, and the
+                              stopped search resumes from its queue head when a slot frees up.
+                              Results do not change; a short request need not wait for a long
+                              launch to end */
 } pg_server_params;
 
 typedef struct {
@@ -353,6 +361,7 @@ typedef struct {
     double sieve_ms;         /* device time of the sieves, summed over launches */
     double prp_ms;           /* device time of the searches, summed over launches */
     double busy_s;           /* wall time with at least one launch in flight */
+    uint64_t preemptions;    /* launches stopped to let waiting windows run (resumed later) */
 } pg_server_stats;
 
 /* Starts a server (and its worker thread) on CUDA device `device`. */

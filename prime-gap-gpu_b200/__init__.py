@@ -122,7 +122,7 @@ class ServerParams(ctypes.Structure):
         ("hbm_budget", ctypes.c_uint64), ("batch_m", ctypes.c_uint32), ("window_m", ctypes.c_uint32),
         ("max_windows", ctypes.c_uint32), ("max_sl", ctypes.c_uint32), ("small_limit", ctypes.c_uint32),
         ("ext_window", ctypes.c_uint32), ("tpi", ctypes.c_uint32), ("warps_per_sm", ctypes.c_uint32),
-        ("slots", ctypes.c_uint32), ("pad", ctypes.c_uint32),
+        ("slots", ctypes.c_uint32), ("preempt_us", ctypes.c_uint32),
     ]
 
 
@@ -147,6 +147,7 @@ class ServerStats(ctypes.Structure):
         ("launches", ctypes.c_uint64), ("windows", ctypes.c_uint64), ("tables_built", ctypes.c_uint64),
         ("tables_evicted", ctypes.c_uint64), ("resident_bytes", ctypes.c_uint64), ("peak_bytes", ctypes.c_uint64),
         ("sieve_ms", ctypes.c_double), ("prp_ms", ctypes.c_double), ("busy_s", ctypes.c_double),
+        ("preemptions", ctypes.c_uint64),
     ]
 
 
@@ -473,9 +474,9 @@ class Server:
 
     def __init__(self, device: int = 0, hbm_budget: int = 0, batch_m: int = 0, window_m: int = 0,
                  max_windows: int = 0, max_sl: int = 0, small_limit: int = 0, ext_window: int = 0, tpi: int = 0,
-                 warps_per_sm: int = 0, slots: int = 0):
+                 warps_per_sm: int = 0, slots: int = 0, preempt_us: int = 0):
         self.params = ServerParams(hbm_budget, batch_m, window_m, max_windows, max_sl, small_limit, ext_window,
-                                   tpi, warps_per_sm, slots, 0)
+                                   tpi, warps_per_sm, slots, preempt_us)
         h = ctypes.c_void_p()
         _check(lib.pg_server_create(device, ctypes.byref(self.params), ctypes.byref(h)))
         self._h = h

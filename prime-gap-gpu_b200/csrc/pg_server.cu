@@ -22,6 +22,15 @@
 // one, so the host work of step 2 overlaps the device; the worker polls the
 // running launch's stream so requests that arrive meanwhile go into a free
 // slot at once.
+//
+// Preemption (pg_server_params.preempt_us): one slot is kept free of running
+// launches.  When windows have waited preempt_us and the longest-running
+// launch has run as long, its persistent search is told to stop (a flag in
+// mapped host memory the warps read between test rounds); the warps leave
+// after the tests in hand, finalize skips the launch, and the slot keeps the
+// search's device state (SUSPENDED).  The waiting windows take the free slot;
+// a suspended launch is resumed from its queue head (the same kernel, same
+// arguments) once fewer than slots - 1 launches run.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -91,7 +100,10 @@ struct SlotState {
     Slot s;
     std::vector<Placed> placed;
     std::vector<const Tables *> tabs;  // table sets the launch reads
-    bool inflight = false;
+    bool inflight = false;   // work enqueued on the slot's stream
+    bool stopping = false;   // its stop flag is raised
+    bool suspended = false;  // its search stopped with items queued: resumed later
+    double t_run = 0;        // when the launch (or its resume) was enqueued
     uint64_t seq = 0;
 };
 
@@ -168,7 +180,8 @@ struct pg_server {
     // set is not evicted until the launch has finished.
     bool read_in_flight(const Tables *T) const {
         for (const auto &ss : slot)
-            if (ss.inflight && std::find(ss.tabs.begin(), ss.tabs.end(), T) != ss.tabs.end()) return true;
+            if ((ss.inflight || ss.suspended) && std::find(ss.tabs.begin(), ss.tabs.end(), T) != ss.tabs.end())
+                return true;
         return false;
     }
 
@@ -370,6 +383,8 @@ struct pg_server {
         }
         ss.placed.clear();
         ss.inflight = false;
+        ss.stopping = false;
+        ss.suspended = false;
     }
 
     // Scatters a finished launch's gaps (step 3).
@@ -397,17 +412,58 @@ struct pg_server {
         ss.inflight = false;
     }
 
+    // launches occupying the device (running or being stopped)
+    size_t running() const {
+        size_t n = 0;
+        for (const auto &ss : slot) n += ss.inflight;
+        return n;
+    }
+
+    // Submit time of the oldest admitted request with windows not yet placed
+    // (< 0 if none).
+    double oldest_waiting() const {
+        double t = -1;
+        for (uint64_t id : order) {
+            const Request &r = reqs.at(id);
+            if (r.state == St::ADMITTED && r.next_m < r.m_end && (t < 0 || r.t_submit < t)) t = r.t_submit;
+        }
+        return t;
+    }
+
+    // Raises the stop flag of the longest-running launch when windows have
+    // waited preempt_us, a slot is free for them, and no launch is stopping.
+    void maybe_preempt() {
+        if (!prm.preempt_us) return;
+        const double wait_since = oldest_waiting();
+        const double limit = prm.preempt_us * 1e-6, t = now();
+        if (wait_since < 0 || t - wait_since < limit) return;
+        bool idle = false;
+        SlotState *victim = nullptr;
+        for (auto &ss : slot) {
+            if (ss.stopping) return;
+            idle |= !ss.inflight && !ss.suspended;
+            if (ss.inflight && t - ss.t_run >= limit && (!victim || ss.t_run < victim->t_run)) victim = &ss;
+        }
+        if (!idle || !victim) return;
+        slot_preempt(victim->s);
+        victim->stopping = true;
+        st.preemptions++;
+    }
+
     void run() {
         cudaSetDevice(ctx->device);
         std::unique_lock<std::mutex> lk(mu);
         double busy_since = -1;
+        const size_t run_limit = prm.preempt_us ? slot.size() - 1 : slot.size();
         while (true) {
             if (!stop) admit(lk);
-            // step 2: every idle slot gets a launch
+            // step 2: idle slots get launches while fewer than run_limit run
             for (auto &ss : slot) {
-                if (ss.inflight || stop) continue;
+                if (ss.inflight || ss.suspended || stop) continue;
+                if (running() >= run_limit) break;
                 if (!fill(ss)) break;
                 ss.seq = ++launch_seq;
+                ss.t_run = now();
                 int rc = slot_enqueue(ss.s, PG_SEARCH_PERSISTENT, PG_SUBMIT_WARPS_PER_SM(prm.warps_per_sm), false);
                 if (rc) {
                     fail_launch(lk, ss, rc, pg_last_error());
@@ -416,28 +472,55 @@ struct pg_server {
                 ss.inflight = true;
                 if (busy_since < 0) busy_since = now();
             }
-            // step 3: finish the oldest launch once its stream is idle; until
-            // then keep admitting and filling as requests arrive
-            SlotState *oldest = nullptr;
-            for (auto &ss : slot)
-                if (ss.inflight && (!oldest || ss.seq < oldest->seq)) oldest = &ss;
-            if (oldest) {
-                const cudaError_t q = cudaStreamQuery(oldest->s.st);
-                if (q == cudaErrorNotReady) {
-                    if (cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();
-                    cv_work.wait_for(lk, std::chrono::microseconds(200));
+            if (!stop && running() >= run_limit) maybe_preempt();
+            // resume stopped launches, oldest first, while there is room
+            while (running() < run_limit) {
+                SlotState *next = nullptr;
+                for (auto &ss : slot)
+                    if (ss.suspended && (!next || ss.seq < next->seq)) next = &ss;
+                if (!next) break;
+                next->suspended = false;
+                next->t_run = now();
+                const int rc = slot_resume(next->s);
+                if (rc) {
+                    fail_launch(lk, *next, rc, pg_last_error());
                     continue;
                 }
+                next->inflight = true;
+                if (busy_since < 0) busy_since = now();
+            }
+            // step 3: finish a launch whose stream is idle (oldest first); until
+            // then keep admitting and filling as requests arrive
+            SlotState *ready = nullptr;
+            bool any_inflight = false;
+            for (auto &ss : slot) {
+                if (!ss.inflight) continue;
+                any_inflight = true;
+                if (ready && ss.seq > ready->seq) continue;
+                const cudaError_t q = cudaStreamQuery(ss.s.st);
+                if (q == cudaErrorNotReady) {
+                    if (cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();
+                    continue;
+                }
+                ready = &ss;
+            }
+            if (ready) {
                 lk.unlock();
-                const int rc = slot_finish(oldest->s);
-                const std::string err = rc ? pg_last_error() : "";
+                const int rc = slot_finish(ready->s);
+                const std::string err = rc < 0 ? pg_last_error() : "";
                 lk.lock();
-                if (rc)
-                    fail_launch(lk, *oldest, rc, err);
-                else
-                    deliver(*oldest);
+                ready->inflight = false;
+                ready->stopping = false;
+                if (rc == SLOT_STOPPED) {
+                    ready->suspended = true;  // holds its state until resumed
+                } else if (rc) {
+                    ready->inflight = true;   // fail_launch drains the stream and frees the slot
+                    fail_launch(lk, *ready, rc, err);
+                } else {
+                    deliver(*ready);
+                }
                 bool any = false;
-                for (auto &ss : slot) any |= ss.inflight;
+                for (auto &ss : slot) any |= ss.inflight || ss.suspended;
                 if (!any && busy_since >= 0) {
                     st.busy_s += now() - busy_since;
                     busy_since = -1;
@@ -445,6 +528,13 @@ struct pg_server {
                 note_bytes();
                 continue;
             }
+            if (any_inflight) {
+                cv_work.wait_for(lk, std::chrono::microseconds(200));
+                continue;
+            }
+            bool suspended = false;
+            for (auto &ss : slot) suspended |= ss.suspended;
+            if (suspended) continue;  // resumed above on the next pass
             if (stop) break;
             bool work = false;
             for (uint64_t id : order) {
@@ -470,8 +560,9 @@ extern "C" int pg_server_create(int device, const pg_server_params *params, pg_s
     if (!p.ext_window) p.ext_window = 64;
     if (p.max_windows > 65535) return fail(PG_ERR_ARG, "max_windows=%u > 65535", p.max_windows);
     if (p.max_sl / 2 > 65535) return fail(PG_ERR_ARG, "max_sl=%u > 131071", p.max_sl);
-    if (!p.slots) p.slots = 2;
+    if (!p.slots) p.slots = p.preempt_us ? 3 : 2;
     if (p.slots > 8) return fail(PG_ERR_ARG, "slots=%u > 8", p.slots);
+    if (p.preempt_us && p.slots < 2) return fail(PG_ERR_ARG, "preemption needs at least 2 slots");
     pg_ctx *c = nullptr;
     int rc = pg_ctx_create(device, &c);
     if (rc) return rc;
@@ -503,6 +594,14 @@ extern "C" int pg_server_create(int device, const pg_server_params *params, pg_s
             return fail(rc, "%s", keep.c_str());
         }
         srv->slot_bytes += ss.s.bytes;
+        if (p.preempt_us && !rc) rc = slot_enable_preempt(ss.s);
+        if (rc) {
+            std::string keep = pg_last_error();
+            for (auto &s2 : srv->slot) slot_free(s2.s);
+            pg_ctx_destroy(c);
+            delete srv;
+            return fail(rc, "%s", keep.c_str());
+        }
     }
     if (srv->slot_bytes > p.hbm_budget) {
         for (auto &ss : srv->slot) slot_free(ss.s);

@@ -34,9 +34,13 @@ def _alone(pg, p, d, sl, limit, m0, minc, rounds):
         return job.search(m0, minc)
 
 
-def test_mixed_requests_equal_alone(pg):
+@pytest.mark.parametrize("preempt_us", [0, 1])
+def test_mixed_requests_equal_alone(pg, preempt_us):
+    """Each request's gaps equal its search alone, batched with the others; with preempt_us = 1 the server
+    stops a running launch whenever windows wait and a slot is free, so launches are stopped and resumed
+    from their queue heads many times."""
     want = [_alone(pg, *r) for r in MIX]
-    with pg.Server(batch_m=6_000, window_m=4_000, max_windows=8, max_sl=8_000) as srv:
+    with pg.Server(batch_m=6_000, window_m=4_000, max_windows=8, max_sl=8_000, preempt_us=preempt_us) as srv:
         ids = [srv.submit(p, d, sl, lim, m0, minc, rounds) for p, d, sl, lim, m0, minc, rounds in MIX]
         got = {i: srv.wait(i) for i in reversed(ids)}
         st = srv.stats()
@@ -50,6 +54,7 @@ def test_mixed_requests_equal_alone(pg):
     assert st["m_done"] == sum(len(w.ms) for w in want)
     assert st["windows"] > st["launches"]          # launches carried several windows
     assert st["tables_built"] == 6                 # one set per (p, d, max_prime)
+    assert (st["preemptions"] > 0) == (preempt_us > 0)
 
 
 def test_requests_from_threads_and_next_done(pg):
