@@ -319,6 +319,29 @@ def run_config(pg, ctx, w: dict) -> dict:
         job.close()
 
 
+PRP_SIZES = (512, 1024, 1536, 4352)  # the reference's BITS builds (gpu_state_and_checks, gpu_testing.cu:369-386)
+
+
+def prp_rates(pg, ctx) -> dict:
+    """Strong base-2 PRP tests per second of pg_prp_batch on random odd numbers of each operand size (one
+    test per number, automatic layout), for comparison with the reference's per-size rates
+    (gpu_testing.cu:65-100: 1 085 K PRP/s at 701#, ~1024 bits, TPI 8 on an A100)."""
+    import numpy as np
+    rng = np.random.default_rng(9)
+    out = {}
+    for bits in PRP_SIZES:
+        words = bits // 32
+        n = max(2048, (1 << 38) // (bits * bits))  # about the same device time at every size
+        a = rng.integers(0, 2**32, size=(n, words), dtype=np.uint64).astype(np.uint32)
+        a[:, 0] |= 1
+        a[:, -1] = (a[:, -1] >> 2) | (1 << 29)  # bits - 2 bits: two spare bits for the lane-group layouts
+        ctx.prp_words(a[:256], 1)  # warm-up
+        t = time.perf_counter()
+        ctx.prp_words(a, 1)
+        out[str(bits)] = {"numbers": n, "tests_per_sec": n / (time.perf_counter() - t)}
+    return out
+
+
 def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
     import torch
     import __graft_entry__
@@ -451,13 +474,15 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
     hbm, hbm_src = hbm_peak()
     esz = 8 if W["max_prime"] >= 2 ** 32 else 4
     table_b = job.info["num_primes"] * 3 * esz
+    walk_b = job.info["num_primes"] * 8 if W["max_prime"] < 2 ** 32 else 0  # sa, sb of every large prime
     rows_b = m_count * job.info["words_per_m"] * 4
-    sieve_b = table_b + 2 * rows_b + survivors * 2
+    sieve_b = table_b + walk_b + 2 * rows_b + survivors * 2
     sieve = {"bound": "hbm", "achieved": sieve_b / (sieve_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
              "frac": sieve_b / (sieve_ms / 1e3) / 1e9 / hbm, "ms_per_window": sieve_ms,
              "bytes_per_window": sieve_b,
              "work": f"prime table {table_b / 1e9:.3f} GB ({job.info['num_primes']} primes x 3 x {esz} B, read "
-                     f"once) + rows {rows_b / 1e6:.1f} MB written and read once + {survivors} survivors x 2 B; "
+                     f"once) + walk table {walk_b / 1e9:.3f} GB (2 x u32 per prime, read once) + rows "
+                     f"{rows_b / 1e6:.1f} MB written and read once + {survivors} survivors x 2 B; "
                      "time = sieve kernels of a window alone (large-prime search, small-prime tiles and lists)",
              "peak_source": hbm_src}
     line = {
@@ -493,6 +518,7 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
     job.close()
     if world == 1 and not args.no_extra:
         line["configs"] = {name: run_config(pg, ctx, w) for name, w in EXTRA.items()}
+        line["configs"]["prp_rates"] = prp_rates(pg, ctx)
         ctx.close()
         line["configs"]["serving"] = run_serve(args, n_jobs=64, compact=True, preempt=0)
         line["configs"]["serving_preempt"] = run_serve(args, n_jobs=64, compact=True, preempt=SERVE_PREEMPT_US)

@@ -274,7 +274,8 @@ int pg_autotune(pg_ctx *ctx, const pg_job_params *base, uint64_t m_start, uint64
  *   2. the small-prime bound of the shared-memory sieve tile: 16384, 65536,
  *      262144;
  *   3. the PRP kernel's warps per SM (PG_SUBMIT_WARPS_PER_SM): 0 (all that
- *      fit), 4, 6, 8, 10, 12;
+ *      fit), 4, 6, 8, 10, 12; the two fastest are timed again, in turn, with
+ *      2 x reps passes each (twice), and the faster on those decides;
  *   4. with PG_TUNE_WINDOW, the m per window: m_inc, m_inc / 2, m_inc / 4.
  * The exponentiation window has no knob: the base-2 test multiplies by
  * doublings, never by a table entry.  Each setting runs one warm-up pass and
@@ -320,14 +321,15 @@ typedef struct {
                               launches in flight share the SMs; 0 = as many as fit */
     uint32_t slots;        /* launch slots (own stream and buffers each); 0 = 2 (3 with preemption),
                               at most 8 */
-    uint32_t preempt_us;   /* preemption of running launches: 0 = off.  Otherwise at most slots - 1
-                              launches run; once windows have waited preempt_us microseconds and a
-                              launch has run as long, that launch's persistent search is told to
-                              stop (its warps leave after the tests in hand), its slot holds the
-                              search's state, the waiting windows run in the free slot, and the
-                              stopped search resumes from its queue head when a slot frees up.
-                              Results do not change; a short request need not wait for a long
-                              launch to end */
+    uint32_t preempt_us;   /* preemption of running launches: 0 = off.  Otherwise launches are
+                              scheduled by operand width, narrowest first, and at most slots - 1 run;
+                              once narrower windows have waited preempt_us microseconds, every
+                              running launch of wider operands is told to stop (its warps leave after
+                              the tests in hand), its slot holds the search's state, the narrower
+                              windows run, and the stopped search resumes from its queue head when
+                              no narrower work runs or waits.  A request waiting max(2 s,
+                              100 x preempt_us) goes first whatever its width.  Results do not
+                              change; a short request need not wait for a long launch to end */
 } pg_server_params;
 
 typedef struct {

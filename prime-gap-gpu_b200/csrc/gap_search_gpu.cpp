@@ -10,8 +10,9 @@
 //   --ranges R    windows of --minc m to search; 0 = until Ctrl-C (the reference's only mode)
 //   --chunk C     m per device call (default min(minc, 1,000,000))
 //   --form persistent|plain   --rounds R   --device N
-//   --warps-per-sm W   cap on each window's PRP warps per SM (default 6; 0 = all that fit):
-//                      two windows are in flight and share the SMs
+//   --warps-per-sm W   cap on each window's PRP warps per SM (default 6 for one-thread operands,
+//                      none for lane-group operands; 0 = all that fit): two windows are in flight
+//                      and share the SMs
 //   --resume FILE      after every finished range write "P D MINC NEXT_MSTART RANGES_DONE" to FILE;
 //                      when FILE exists at start (same P, D, MINC), continue from it
 //   --devices A,B,...  one worker per listed CUDA device, each searching whole ranges (the m ranges
@@ -65,7 +66,7 @@ struct Config {
     int form = PG_SEARCH_PERSISTENT;
     uint32_t rounds = 1;
     int device = 0;
-    uint32_t warps_per_sm = 6;
+    int warps_per_sm = -1;  // -1: 6 for one-thread layouts, no cap for lane groups
     std::string resume;
     std::vector<int> devices;  // --devices; empty = {device}
     uint32_t confirm_rounds = 16;
@@ -83,7 +84,7 @@ static void show_usage(const char *name) {
     printf("  --chunk <C>     m per device call (default min(minc, 1000000))\n");
     printf("  --form persistent|plain   --rounds <bases>   --device <n>\n");
     printf("  --warps-per-sm <W>  PRP warps per SM of each of the two windows in flight\n");
-    printf("                      (default 6, 0 = as many as fit)\n");
+    printf("                      (default 6, or all for lane-group operands; 0 = as many as fit)\n");
     printf("  --resume <file>     progress file: written after every finished range, read at start\n");
     printf("  --devices <a,b,..>  search on these CUDA devices, one range per device at a time\n");
     printf("  --confirm-rounds <R> strong bases both primes of a record pass (default 16, 0 = off)\n");
@@ -140,7 +141,7 @@ static Config argparse(int argc, char **argv) {
                 break;
             case 24: c.rounds = (uint32_t)atoi(optarg); break;
             case 25: c.device = atoi(optarg); break;
-            case 26: c.warps_per_sm = (uint32_t)atoi(optarg); break;
+            case 26: c.warps_per_sm = atoi(optarg); break;
             case 27: c.resume = optarg; break;
             case 28:
                 for (const char *q = optarg; *q;) {
@@ -311,7 +312,10 @@ static int search_range(Engine &e, const Config &c, uint64_t chunk, uint64_t m_s
         uint64_t ticket;
         int buf;
     };
-    const uint32_t flags = c.form == PG_SEARCH_PERSISTENT ? PG_SUBMIT_WARPS_PER_SM(c.warps_per_sm) : 0u;
+    // default cap: two one-thread windows in flight share the SMs best at 6 warps per SM each; the lane
+    // groups' carry chains need all the warps their registers allow to hide their latency
+    const uint32_t wps = c.warps_per_sm >= 0 ? (uint32_t)c.warps_per_sm : (e.info.tpi > 1 ? 0u : 6u);
+    const uint32_t flags = c.form == PG_SEARCH_PERSISTENT ? PG_SUBMIT_WARPS_PER_SM(wps) : 0u;
     std::vector<Pending> pending;
     auto finish_one = [&]() {
         const Pending pd = pending.front();

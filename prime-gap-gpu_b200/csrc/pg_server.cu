@@ -11,7 +11,8 @@
 //      request uses them) least recently used first; a request whose tables
 //      cannot fit waits, or fails when nothing else holds memory.
 //   2. fill every idle slot with one search launch: the operand layout of
-//      the oldest admitted request with windows left, then windows of every
+//      the oldest admitted request with windows left (with preemption: of the
+//      cheapest class with windows left), then windows of every
 //      admitted request of that layout in arrival order until the slot is
 //      full (coprime m, windows, list space).  Windows of different requests
 //      (different K, sl, rounds) share the launch; the kernels read each
@@ -23,14 +24,18 @@
 // running launch's stream so requests that arrive meanwhile go into a free
 // slot at once.
 //
-// Preemption (pg_server_params.preempt_us): one slot is kept free of running
-// launches.  When windows have waited preempt_us and the longest-running
-// launch has run as long, its persistent search is told to stop (a flag in
-// mapped host memory the warps read between test rounds); the warps leave
-// after the tests in hand, finalize skips the launch, and the slot keeps the
-// search's device state (SUSPENDED).  The waiting windows take the free slot;
-// a suspended launch is resumed from its queue head (the same kernel, same
-// arguments) once fewer than slots - 1 launches run.
+// Preemption (pg_server_params.preempt_us): launches are scheduled by
+// operand class (words per number; a test costs ~ words^2 x bits), cheapest
+// first, and one slot is kept free of running launches.  A persistent launch
+// holds every SM it fits on until its queue drains, so once cheaper windows
+// have waited preempt_us (or a cheaper launch has been in flight that long),
+// every running launch of a costlier class is told to stop (a flag in mapped
+// host memory the warps read between test rounds); its warps leave after the
+// tests in hand, finalize skips the launch, and the slot keeps the search's
+// device state (SUSPENDED).  A suspended launch resumes from its queue head
+// (the same kernel, same arguments) when fewer than slots - 1 launches run
+// and no cheaper work runs or waits.  A request that has waited
+// max(2 s, 100 x preempt_us) is placed first whatever its class.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -135,6 +140,7 @@ struct pg_server {
     uint64_t next_id = 1;
     std::map<uint64_t, Request> reqs;   // every request not yet waited for
     std::deque<uint64_t> order;         // queued / admitted ids in arrival order
+    double aging_s = 0;                 // with preemption: a request waiting this long goes first
     std::deque<uint64_t> done_ids;      // finished, not yet returned by next_done
     std::map<TableKey, TableEntry> tables;
     uint64_t admissions = 0;
@@ -302,20 +308,43 @@ struct pg_server {
         }
     }
 
+    // Scheduling class of an operand layout: its words (a test costs ~ words^2 x bits).
+    static uint32_t cls(uint32_t layout) { return layout_words(layout); }
+
+    // The layout the next launch packs (0: no windows wait) and the submit
+    // time of its oldest waiting request.  Without preemption: the oldest
+    // waiting request's.  With it: the cheapest class with windows waiting,
+    // so short requests overtake long ones, unless the oldest waiting request
+    // has waited aging_s, which then goes first.
+    uint32_t next_layout(double *since = nullptr) const {
+        uint32_t best = 0;
+        double t_best = -1;
+        bool first = true;
+        for (uint64_t id : order) {
+            const Request &r = reqs.at(id);
+            if (r.state != St::ADMITTED || r.next_m >= r.m_end) continue;
+            if (first && (!prm.preempt_us || now() - r.t_submit >= aging_s)) {
+                best = r.job->L;
+                t_best = r.t_submit;
+                break;
+            }
+            first = false;
+            if (!best || cls(r.job->L) < cls(best)) {
+                best = r.job->L;
+                t_best = r.t_submit;
+            }
+        }
+        if (since) *since = t_best;
+        return best;
+    }
+
     // Packs windows into an idle slot (step 2); false when there is no work.
     bool fill(SlotState &ss) {
         Slot &s = ss.s;
         slot_reset(s);
         ss.placed.clear();
         ss.tabs.clear();
-        uint32_t layout = 0;
-        for (uint64_t id : order) {
-            const Request &r = reqs.at(id);
-            if (r.state == St::ADMITTED && r.next_m < r.m_end) {
-                layout = r.job->L;
-                break;
-            }
-        }
+        const uint32_t layout = next_layout();
         if (!layout) return false;
         std::vector<std::pair<uint64_t, std::pair<int, std::string>>> failed;
         for (uint64_t id : order) {
@@ -419,35 +448,50 @@ struct pg_server {
         return n;
     }
 
-    // Submit time of the oldest admitted request with windows not yet placed
-    // (< 0 if none).
-    double oldest_waiting() const {
-        double t = -1;
-        for (uint64_t id : order) {
-            const Request &r = reqs.at(id);
-            if (r.state == St::ADMITTED && r.next_m < r.m_end && (t < 0 || r.t_submit < t)) t = r.t_submit;
-        }
-        return t;
-    }
-
-    // Raises the stop flag of the longest-running launch when windows have
-    // waited preempt_us, a slot is free for them, and no launch is stopping.
+    // With preemption: a persistent launch holds every SM it fits on until its
+    // queue drains, so cheaper work would wait behind it.  Once a launch of a
+    // cheaper class has been in flight preempt_us, or the next launch's
+    // windows (next_layout) have waited preempt_us with a slot free for them,
+    // raise the stop flag of every running launch of a costlier class.
     void maybe_preempt() {
         if (!prm.preempt_us) return;
-        const double wait_since = oldest_waiting();
         const double limit = prm.preempt_us * 1e-6, t = now();
-        if (wait_since < 0 || t - wait_since < limit) return;
+        uint32_t c = UINT32_MAX;  // cheapest class that has waited long enough
         bool idle = false;
-        SlotState *victim = nullptr;
-        for (auto &ss : slot) {
-            if (ss.stopping) return;
+        for (const auto &ss : slot) {
             idle |= !ss.inflight && !ss.suspended;
-            if (ss.inflight && t - ss.t_run >= limit && (!victim || ss.t_run < victim->t_run)) victim = &ss;
+            if (ss.inflight && !ss.stopping && t - ss.t_run >= limit) c = std::min(c, cls(ss.s.L));
         }
-        if (!idle || !victim) return;
-        slot_preempt(victim->s);
-        victim->stopping = true;
-        st.preemptions++;
+        double since = -1;
+        const uint32_t L = next_layout(&since);
+        if (L && idle && t - since >= limit) c = std::min(c, cls(L));
+        if (c == UINT32_MAX) return;
+        for (auto &ss : slot) {
+            if (!ss.inflight || ss.stopping || cls(ss.s.L) <= c) continue;
+            slot_preempt(ss.s);
+            ss.stopping = true;
+            st.preemptions++;
+        }
+    }
+
+    // A stopped launch resumes when no launch of a cheaper class runs and,
+    // unless the server is stopping, no windows of a cheaper class wait.
+    bool may_resume(const SlotState &x) const {
+        for (const auto &ss : slot)
+            if (ss.inflight && cls(ss.s.L) < cls(x.s.L)) return false;
+        if (stop) return true;
+        const uint32_t L = next_layout();
+        return !L || cls(L) >= cls(x.s.L);
+    }
+
+    // An idle slot takes new windows unless a stopped launch of the same or a
+    // cheaper class waits to resume (it goes first).
+    bool may_fill() const {
+        const uint32_t L = next_layout();
+        if (!L) return false;
+        for (const auto &ss : slot)
+            if (ss.suspended && cls(ss.s.L) <= cls(L)) return false;
+        return true;
     }
 
     void run() {
@@ -457,27 +501,11 @@ struct pg_server {
         const size_t run_limit = prm.preempt_us ? slot.size() - 1 : slot.size();
         while (true) {
             if (!stop) admit(lk);
-            // step 2: idle slots get launches while fewer than run_limit run
-            for (auto &ss : slot) {
-                if (ss.inflight || ss.suspended || stop) continue;
-                if (running() >= run_limit) break;
-                if (!fill(ss)) break;
-                ss.seq = ++launch_seq;
-                ss.t_run = now();
-                int rc = slot_enqueue(ss.s, PG_SEARCH_PERSISTENT, PG_SUBMIT_WARPS_PER_SM(prm.warps_per_sm), false);
-                if (rc) {
-                    fail_launch(lk, ss, rc, pg_last_error());
-                    continue;
-                }
-                ss.inflight = true;
-                if (busy_since < 0) busy_since = now();
-            }
-            if (!stop && running() >= run_limit) maybe_preempt();
             // resume stopped launches, oldest first, while there is room
             while (running() < run_limit) {
                 SlotState *next = nullptr;
                 for (auto &ss : slot)
-                    if (ss.suspended && (!next || ss.seq < next->seq)) next = &ss;
+                    if (ss.suspended && may_resume(ss) && (!next || ss.seq < next->seq)) next = &ss;
                 if (!next) break;
                 next->suspended = false;
                 next->t_run = now();
@@ -489,6 +517,22 @@ struct pg_server {
                 next->inflight = true;
                 if (busy_since < 0) busy_since = now();
             }
+            // step 2: idle slots get launches while fewer than run_limit run
+            for (auto &ss : slot) {
+                if (ss.inflight || ss.suspended || stop) continue;
+                if (running() >= run_limit || !may_fill()) break;
+                if (!fill(ss)) break;
+                ss.seq = ++launch_seq;
+                ss.t_run = now();
+                int rc = slot_enqueue(ss.s, PG_SEARCH_PERSISTENT, PG_SUBMIT_WARPS_PER_SM(prm.warps_per_sm), false);
+                if (rc) {
+                    fail_launch(lk, ss, rc, pg_last_error());
+                    continue;
+                }
+                ss.inflight = true;
+                if (busy_since < 0) busy_since = now();
+            }
+            if (!stop) maybe_preempt();
             // step 3: finish a launch whose stream is idle (oldest first); until
             // then keep admitting and filling as requests arrive
             SlotState *ready = nullptr;
@@ -576,6 +620,7 @@ extern "C" int pg_server_create(int device, const pg_server_params *params, pg_s
     srv->prm = p;
     srv->t0 = std::chrono::steady_clock::now();
     srv->slot.resize(p.slots);
+    srv->aging_s = std::max(2.0, 1e-4 * p.preempt_us);
     // launch capacities: batch_m coprime m over at most max_windows windows
     // of window_m m; lists at most half of each side's positions
     const uint64_t nodd_w = p.window_m / 2 + 1;

@@ -5,6 +5,7 @@ from __future__ import annotations
 
 import math
 import threading
+import time
 
 import numpy as np
 import pytest
@@ -36,12 +37,18 @@ def _alone(pg, p, d, sl, limit, m0, minc, rounds):
 
 @pytest.mark.parametrize("preempt_us", [0, 1])
 def test_mixed_requests_equal_alone(pg, preempt_us):
-    """Each request's gaps equal its search alone, batched with the others; with preempt_us = 1 the server
-    stops a running launch whenever windows wait and a slot is free, so launches are stopped and resumed
-    from their queue heads many times."""
+    """Each request's gaps equal its search alone, batched with the others.  The requests arrive widest
+    operands first, a class every 0.3 s, so with preempt_us = 1 each narrower class stops the wider
+    launches still running (the P=3001 launch runs over a second) and they resume from their queue heads
+    once the narrower work is done."""
     want = [_alone(pg, *r) for r in MIX]
     with pg.Server(batch_m=6_000, window_m=4_000, max_windows=8, max_sl=8_000, preempt_us=preempt_us) as srv:
-        ids = [srv.submit(p, d, sl, lim, m0, minc, rounds) for p, d, sl, lim, m0, minc, rounds in MIX]
+        ids = [0] * len(MIX)
+        arrival = sorted(range(len(MIX)), key=lambda i: -MIX[i][0])
+        for k, i in enumerate(arrival):
+            if k and MIX[i][0] != MIX[arrival[k - 1]][0]:
+                time.sleep(0.3)
+            ids[i] = srv.submit(*MIX[i])
         got = {i: srv.wait(i) for i in reversed(ids)}
         st = srv.stats()
     for i, w in zip(ids, want):
