@@ -126,7 +126,9 @@ typedef struct {
 #define PG_JOB_LARGE_STEP   0x1u   /* step every X for every prime */
 #define PG_JOB_LARGE_SEARCH 0x2u   /* modular search for the next hit */
 #define PG_JOB_NO_GRAPH     0x4u   /* launch the persistent form's kernels one by one
-                                      instead of as one CUDA graph per window */
+                                      instead of as one CUDA graph per window; pg_job_create
+                                      then returns without waiting for the device (the job's
+                                      launches wait for its set-up on their own streams) */
 #define PG_JOB_COMPACT_WALK 0x8u   /* keep the large-prime sieve's walk steps (8 B per prime below
                                       2^32, computed at job creation: 0.8 GB at 2e9) only for the
                                       primes expecting >= 64 hits per window; the others find each
@@ -274,8 +276,9 @@ int pg_autotune(pg_ctx *ctx, const pg_job_params *base, uint64_t m_start, uint64
  *   2. the small-prime bound of the shared-memory sieve tile: 16384, 65536,
  *      262144;
  *   3. the PRP kernel's warps per SM (PG_SUBMIT_WARPS_PER_SM): 0 (all that
- *      fit), 4, 6, 8, 10, 12; the two fastest are timed again, in turn, with
- *      2 x reps passes each (twice), and the faster on those decides;
+ *      fit), 4, 6, 8, 10, 12, each over max(2 x reps, 8) passes (a short
+ *      sample favours full occupancy), then the two fastest once more, and
+ *      the mean of their two timings decides;
  *   4. with PG_TUNE_WINDOW, the m per window: m_inc, m_inc / 2, m_inc / 4.
  * The exponentiation window has no knob: the base-2 test multiplies by
  * doublings, never by a table entry.  Each setting runs one warm-up pass and
@@ -287,7 +290,8 @@ typedef struct {
     uint32_t warps_per_sm;  /* the chosen PG_SUBMIT_WARPS_PER_SM cap (0 = as many as fit) */
     uint32_t settings;      /* settings timed */
     uint64_t window_m;      /* the chosen m per window */
-    double m_per_sec;       /* the chosen setting's m/s, PG_SEARCH_SLOTS windows in flight */
+    double m_per_sec;       /* the chosen setting's m/s, PG_SEARCH_SLOTS windows in flight (from
+                               the longer re-timing of the caps, unless a window size won after it) */
     double first_m_per_sec; /* m/s of the first setting timed (tpi 0 with base's knobs, no cap) */
 } pg_tune_result;
 int pg_autotune_ex(pg_ctx *ctx, const pg_job_params *base, uint64_t m_start, uint64_t m_inc, uint32_t flags,
@@ -319,10 +323,11 @@ typedef struct {
     uint32_t tpi;          /* as pg_job_params (0 = automatic) */
     uint32_t warps_per_sm; /* cap on each launch's PRP warps per SM (PG_SUBMIT_WARPS_PER_SM), so the
                               launches in flight share the SMs; 0 = as many as fit */
-    uint32_t slots;        /* launch slots (own stream and buffers each); 0 = 2 (3 with preemption),
-                              at most 8 */
+    uint32_t slots;        /* launch slots (own stream and buffers each); 0 = 2 (4 with preemption:
+                              two run, the others hold stopped launches), at most 8 */
     uint32_t preempt_us;   /* preemption of running launches: 0 = off.  Otherwise launches are
-                              scheduled by operand width, narrowest first, and at most slots - 1 run;
+                              scheduled by operand width, narrowest first, and at most
+                              min(slots - 1, 2) run;
                               once narrower windows have waited preempt_us microseconds, every
                               running launch of wider operands is told to stop (its warps leave after
                               the tests in hand), its slot holds the search's state, the narrower

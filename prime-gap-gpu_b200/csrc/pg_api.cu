@@ -145,7 +145,9 @@ extern "C" int pg_ctx_create(int device, pg_ctx **out) {
     pg_ctx *c = new pg_ctx();
     c->device = device;
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->up, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
+        if (c->stream) cudaStreamDestroy(c->stream);
         delete c;
         return fail(PG_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
     }
@@ -192,6 +194,10 @@ extern "C" int pg_ctx_destroy(pg_ctx *c) {
     cudaFree(c->d_cand);
     cudaFree(c->d_res);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->up) {
+        cudaStreamSynchronize(c->up);
+        cudaStreamDestroy(c->up);
+    }
     delete c;
     return PG_OK;
 }
@@ -510,6 +516,7 @@ void pg::slot_reset(Slot &s) {
     s.stride = 0;
     s.ext_window = 0;
     s.confirm = false;
+    s.fin_active = false;
     s.sst = pg_search_stats{};
 }
 
@@ -630,6 +637,7 @@ static uint64_t seg_bands(const pg_job *j, uint64_t split, uint64_t nodd, SegBan
 static int run_sieve(Slot &s, const WinPart &w, bool compact) {
     const pg_job *j = w.job;
     const pg::Tables &T = *j->T;
+    if (j->ready) PG_CUDA(cudaStreamWaitEvent(s.st, j->ready, 0));
     PG_CUDA(cudaMemsetAsync(s.d_bitmaps, 0, (size_t)w.nm * j->W * 4, s.st));
     LargeArgs la{};
     la.sly = j->sly;
@@ -806,6 +814,7 @@ void pg::slot_preempt(Slot &s) {
 int pg::slot_resume(Slot &s) {
     if (!s.d_stop) return fail(PG_ERR_STATE, "slot_resume: the slot has no stop flag");
     *s.h_stop = 0;
+    s.fin_active = false;
     const uint32_t S = 2 * s.nm;
     PG_CUDA(cudaMemsetAsync(&s.d_sc->stopped, 0, 4, s.st));
     PG_CUDA(launch_search_persistent(s.L, s.search, s.grid, s.st));
@@ -820,6 +829,7 @@ int pg::slot_resume(Slot &s) {
 }
 
 int pg::slot_enqueue(Slot &s, int form, uint32_t flags, bool graph) {
+    s.fin_active = false;
     s.sst.m_count = s.nm;
     s.sst.h2d_bytes = (uint64_t)s.nm * 8 + (uint64_t)s.nodd * 4 + s.parts.size() * sizeof(WinInfo) +
                       (s.parts.size() > 1 ? (uint64_t)s.nm * 2 : 0);
@@ -861,16 +871,22 @@ int pg::slot_enqueue(Slot &s, int form, uint32_t flags, bool graph) {
 // 4x larger extension windows; once every side has a prime, confirms the
 // primes of large gaps (windows with confirm_rounds >= 2) and continues the
 // sides whose prime failed from their next candidate.  Then reads the timings.
-int pg::slot_finish(Slot &s) {
-    PG_CUDA(cudaStreamSynchronize(s.st));
-    if (s.nm == 0) return PG_OK;
-    if (s.h_sc->stopped) return SLOT_STOPPED;  // preempted before its queue ran out: slot_resume
+// Each round is queued on the slot's stream; its results (n_redo, gaps) come
+// back with the Scalars copy, read after the stream is idle.
+int pg::slot_finish(Slot &s, bool wait) {
     const uint32_t S = 2 * s.nm;
-    SearchArgs a = base_args(s);
-    uint32_t ext_done = s.ext_window;
-    for (int round = 0;; round++) {
-        uint32_t n_redo = s.h_sc->n_redo;
-        if (n_redo == 0 && s.confirm) {  // every side resolved: confirm the large gaps
+    while (true) {
+        PG_CUDA(cudaStreamSynchronize(s.st));  // no wait when the caller saw the stream idle
+        if (s.nm == 0) return PG_OK;
+        if (!s.fin_active) {
+            if (s.h_sc->stopped) return SLOT_STOPPED;  // preempted before its queue ran out: slot_resume
+            s.fin_active = true;
+            s.fin_phase = 0;
+            s.fin_round = 0;
+            s.fin_ext = s.ext_window;
+        }
+        const uint32_t n_redo = s.h_sc->n_redo;
+        if (n_redo == 0 && s.fin_phase == 0 && s.confirm) {  // every side resolved: confirm the large gaps
             SearchArgs c = base_args(s);
             c.act = s.d_act0;  // 0 .. S-1
             c.n_act = S;
@@ -882,14 +898,19 @@ int pg::slot_finish(Slot &s) {
             PG_CUDA(cudaMemcpyAsync(s.h_gaps, s.d_gaps, (size_t)S * 4, cudaMemcpyDeviceToHost, s.st));
             PG_CUDA(cudaMemcpyAsync(s.h_sc, s.d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s.st));
             s.sst.d2h_bytes += 4;
-            PG_CUDA(cudaStreamSynchronize(s.st));
-            n_redo = s.h_sc->n_redo;
+            s.fin_phase = 1;
+            if (!wait) return SLOT_PENDING;
+            continue;
         }
         if (n_redo == 0) break;
-        if (round >= 24)
-            return fail(PG_ERR_STATE, "pg_search: %u sides unresolved after %u extension positions", n_redo, ext_done);
+        if (s.fin_round >= 24) {
+            s.fin_active = false;
+            return fail(PG_ERR_STATE, "pg_search: %u sides unresolved after %u extension positions", n_redo,
+                        s.fin_ext);
+        }
+        SearchArgs a = base_args(s);
         PG_CUDA(cudaMemcpyAsync(s.d_act1, s.d_redo, (size_t)n_redo * 4, cudaMemcpyDeviceToDevice, s.st));
-        const uint32_t ext_new = std::min<uint32_t>(ext_done * 4, 1u << 26);
+        const uint32_t ext_new = std::min<uint32_t>(s.fin_ext * 4, 1u << 26);
         a.act = s.d_act1;
         a.n_act = n_redo;
         a.ext_max = ext_new;
@@ -900,7 +921,8 @@ int pg::slot_finish(Slot &s) {
         s.sst.kernel_launches++;
         s.sst.relaunches++;
         s.sst.extended_sides += n_redo;
-        ext_done = ext_new;
+        s.fin_ext = ext_new;
+        s.fin_round++;
         // finalize the continued sides only (their gaps and a new redo list)
         PG_CUDA(cudaMemsetAsync(&s.d_sc->n_redo, 0, 4, s.st));
         PG_CUDA(launch_finalize(s.L, a, S, s.d_gaps, s.d_redo, &s.d_sc->n_redo, &s.d_sc->confirm, s.d_kstart, s.st));
@@ -909,8 +931,10 @@ int pg::slot_finish(Slot &s) {
         PG_CUDA(cudaMemcpyAsync(s.h_gaps, s.d_gaps, (size_t)S * 4, cudaMemcpyDeviceToHost, s.st));
         PG_CUDA(cudaMemcpyAsync(s.h_sc, s.d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s.st));
         s.sst.d2h_bytes += 4;
-        PG_CUDA(cudaStreamSynchronize(s.st));
+        s.fin_phase = 0;
+        if (!wait) return SLOT_PENDING;
     }
+    s.fin_active = false;
     s.sst.d2h_bytes += (uint64_t)S * 4 + sizeof(Scalars);
     float t_sieve = 0, t_prp = 0, t_kernel = 0;
     if (cudaEventElapsedTime(&t_sieve, s.ev[0], s.ev[1]) != cudaSuccess) t_sieve = 0;
@@ -939,6 +963,10 @@ static void job_free(pg_job *j) {
     if (!j) return;
     cudaSetDevice(j->ctx->device);
     cudaStreamSynchronize(j->ctx->stream);
+    if (j->ready) {
+        cudaEventSynchronize(j->ready);
+        cudaEventDestroy(j->ready);
+    }
     for (auto &s : j->slot) slot_free(s);
     cudaFree(j->d_wheel);
     cudaFree(j->d_walk);
@@ -979,8 +1007,22 @@ static int job_build(pg_job *j) {
     for (uint32_t y = 1; y <= j->sly; y++) j->cap += !((wheel[(j->sly + y) >> 5] >> ((j->sly + y) & 31)) & 1u);
     if (j->cap == 0) j->cap = 1;
     if ((rc = dalloc(j->own_bytes, &j->d_wheel, j->W))) return rc;
-    PG_CUDA(cudaMemcpyAsync(j->d_wheel, wheel.data(), wheel.size() * 4, cudaMemcpyHostToDevice, j->ctx->stream));
-    PG_CUDA(cudaStreamSynchronize(j->ctx->stream));
+    // Jobs launched without graphs (the server's, created while other launches
+    // hold the SMs) do not wait for the device: the wheel goes up on the
+    // context's copy-only stream (a pageable copy returns once it is staged),
+    // the walk kernel queues behind it on the context's stream, and every
+    // launch of the job waits for j->ready on its own stream first.
+    const bool async = p.flags & PG_JOB_NO_GRAPH;
+    if (async) {
+        PG_CUDA(cudaEventCreateWithFlags(&j->ready, cudaEventDisableTiming));
+        PG_CUDA(cudaMemcpyAsync(j->d_wheel, wheel.data(), wheel.size() * 4, cudaMemcpyHostToDevice, j->ctx->up));
+        PG_CUDA(cudaEventRecord(j->ready, j->ctx->up));
+        PG_CUDA(cudaStreamWaitEvent(j->ctx->stream, j->ready, 0));
+    } else {
+        PG_CUDA(cudaMemcpyAsync(j->d_wheel, wheel.data(), wheel.size() * 4, cudaMemcpyHostToDevice,
+                                j->ctx->stream));
+        PG_CUDA(cudaStreamSynchronize(j->ctx->stream));
+    }
     // ---- per-window constants
     std::memset(&j->win, 0, sizeof j->win);
     std::memcpy(j->win.K, T.K.data(), T.K.size() * 4);
@@ -1017,9 +1059,10 @@ static int job_build(pg_job *j) {
             if ((rc = dalloc(j->own_bytes, &j->d_walk, j->walk_count))) return rc;
             PG_CUDA(launch_walk_consts(T.d_lp, T.d_lc, T.d_lcinv, T.wide, first, j->walk_count, 2 * j->sly,
                                        j->d_walk, j->ctx->stream));
-            PG_CUDA(cudaStreamSynchronize(j->ctx->stream));
+            if (!async) PG_CUDA(cudaStreamSynchronize(j->ctx->stream));
         }
     }
+    if (async) PG_CUDA(cudaEventRecord(j->ready, j->ctx->stream));  // after the wheel copy and the walk kernel
     return PG_OK;
 }
 
@@ -1314,7 +1357,6 @@ extern "C" int pg_autotune_ex(pg_ctx *c, const pg_job_params *base, uint64_t m_s
     best.params = p;
     best.window_m = m_inc;
     uint32_t settings = 0;
-    double last_v = 0;
     // times job parameters q with warps cap w and window size win; keeps the best
     auto trial = [&](const pg_job_params &q, uint32_t w, uint64_t win) -> int {
         pg_job *j = nullptr;
@@ -1324,7 +1366,6 @@ extern "C" int pg_autotune_ex(pg_ctx *c, const pg_job_params *base, uint64_t m_s
         rc = time_pipelined(j, m_start, m_inc, win, PG_SUBMIT_WARPS_PER_SM(w), reps, &v);
         pg_job_destroy(j);
         if (rc) return rc;
-        last_v = v;
         if (settings++ == 0) best.first_m_per_sec = v;
         if (v > best.m_per_sec) {
             best.m_per_sec = v;
@@ -1356,36 +1397,38 @@ extern "C" int pg_autotune_ex(pg_ctx *c, const pg_job_params *base, uint64_t m_s
         if (rc == PG_ERR_UNSUPPORTED) continue;
         if (rc) return rc;
     }
-    // 3. PRP warps per SM, two windows in flight
-    const uint32_t caps[] = {4, 6, 8, 10, 12};
+    // 3. PRP warps per SM, two windows in flight.  The caps differ by a few
+    // per cent, and a sample of one or two windows favours full occupancy
+    // (its windows start side by side and end alone), so every cap is timed
+    // over at least 8 windows on one job, then the two best once more, and
+    // the mean of their two timings decides.
+    const uint32_t caps[] = {0, 4, 6, 8, 10, 12};
     const pg_job_params tuned = best.params;
-    std::vector<std::pair<double, uint32_t>> by_cap{{best.m_per_sec, 0u}};
-    for (uint32_t w : caps) {
-        const int rc = trial(tuned, w, m_inc);
-        if (rc) return rc;
-        by_cap.push_back({last_v, w});
-    }
-    // 3b. the caps differ by a few per cent, about the noise of one short
-    // timing: the two best are timed again, in turn, with twice the windows
-    std::sort(by_cap.rbegin(), by_cap.rend());
-    if (by_cap.size() >= 2) {
+    {
         pg_job *j = nullptr;
         int rc = pg_job_create(c, &tuned, &j);
         if (rc) return rc;
-        double sum[2] = {0, 0};
-        for (int round = 0; round < 2 && !rc; round++)
-            for (int k = 0; k < 2 && !rc; k++) {
-                double v = 0;
-                rc = time_pipelined(j, m_start, m_inc, m_inc, PG_SUBMIT_WARPS_PER_SM(by_cap[k].second), 2 * reps, &v);
-                sum[k] += v;
-                settings++;
-            }
+        const uint32_t passes = std::max(2 * reps, 8u);
+        std::vector<std::pair<double, uint32_t>> by_cap;
+        for (uint32_t w : caps) {
+            double v = 0;
+            if ((rc = time_pipelined(j, m_start, m_inc, m_inc, PG_SUBMIT_WARPS_PER_SM(w), passes, &v))) break;
+            by_cap.push_back({v, w});
+            settings++;
+        }
+        std::sort(by_cap.rbegin(), by_cap.rend());
+        for (size_t k = 0; k < 2 && !rc; k++) {
+            double v = 0;
+            rc = time_pipelined(j, m_start, m_inc, m_inc, PG_SUBMIT_WARPS_PER_SM(by_cap[k].second), passes, &v);
+            by_cap[k].first = (by_cap[k].first + v) / 2;
+            settings++;
+        }
         pg_job_destroy(j);
         if (rc) return rc;
-        const int k = sum[1] > sum[0] ? 1 : 0;
+        const size_t k = by_cap[1].first > by_cap[0].first ? 1 : 0;
         best.params = tuned;
         best.warps_per_sm = by_cap[k].second;
-        best.m_per_sec = sum[k] / 2;
+        best.m_per_sec = by_cap[k].first;
         best.window_m = m_inc;
     }
     // 4. window size

@@ -25,6 +25,7 @@ namespace pg {
 
 constexpr int SLOT_FULL = 1;
 constexpr int SLOT_STOPPED = 2;  // slot_finish: the search was preempted; slot_resume continues it
+constexpr int SLOT_PENDING = 3;  // slot_finish(wait = false): another round is queued; call again when idle
 
 // records the calling thread's error text and returns code
 int fail(int code, const char *fmt, ...);
@@ -121,6 +122,11 @@ struct Slot {
     volatile uint32_t *h_stop = nullptr;
     uint32_t *d_stop = nullptr;
     SearchArgs search{};
+    // slot_finish's place between calls: after a finalize (0) or a record
+    // confirmation (1); continuation rounds so far; extension positions done
+    bool fin_active = false;
+    int fin_phase = 0;
+    uint32_t fin_round = 0, fin_ext = 0;
     int grid = 0;
     bool busy = false;
     uint64_t ticket = 0;
@@ -143,7 +149,10 @@ bool slot_fits(const Slot &s, const pg_job *j, uint64_t nm, uint64_t nodd);
 int slot_enqueue(Slot &s, int form, uint32_t flags, bool graph);
 // Waits for the queued work, continues unresolved sides past sl, and fills
 // the slot's stats.  Gaps are then in h_gaps (next side 2i, prev side 2i+1).
-int slot_finish(Slot &s);
+// With wait = false it returns SLOT_PENDING after queueing each further round
+// (record confirmation or continuation) instead of waiting for it: call it
+// again once the slot's stream is idle.
+int slot_finish(Slot &s, bool wait = true);
 // Gives the slot a stop flag: its persistent searches can be preempted.
 int slot_enable_preempt(Slot &s);
 // Raises the stop flag of the slot's running search (host write, no call into
@@ -160,6 +169,7 @@ int job_create(pg_ctx *c, const pg_job_params &p, pg_job **out);
 struct pg_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t up = nullptr;  // host-to-device copies only: never queued behind a kernel
     int sms = 0;
     // PRP batch staging
     uint32_t *d_cand = nullptr;
@@ -180,6 +190,9 @@ struct pg_job {
     std::shared_ptr<pg::Tables> T;
     uint32_t L = 0, sly = 0, W = 0, cap = 0;
     uint32_t *d_wheel = nullptr;
+    // jobs built without waiting on the device (PG_JOB_NO_GRAPH): the wheel
+    // and the walk table are in place once this event completes
+    cudaEvent_t ready = nullptr;
     pg::WinInfo win{};  // K, trial residues, sly, rounds
     std::vector<uint8_t> coprime;       // [d] gcd(r, d) == 1
     uint64_t nm_cap = 0, nodd_cap = 0;  // one window of max_m_inc

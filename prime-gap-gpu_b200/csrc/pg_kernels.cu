@@ -366,29 +366,52 @@ struct DivBy<uint64_t> {
 // is W minus the landing value of the level below, so no state is kept on
 // the way down and nothing is rebuilt on the way back; the caller recovers
 // x = (u - B) * A^-1 mod M with one modular product.
+//
+// One level: true with u set when the search ends here, else the next
+// level's (A, B, M) in place (the caller flips the reflection parity).
+template <typename U>
+__device__ __forceinline__ bool modsearch_level(U &A, U &B, U &M, U W, U &u) {
+    if (B <= W) {
+        u = B;
+        return true;
+    }
+    const DivBy<U> by(A);
+    if (W + 1 >= A) {
+        const U t = by.rem(M - B);
+        u = t ? A - t : 0;
+        return true;
+    }
+    const U r = by.rem(M);
+    U b1 = by.rem(B);
+    b1 = b1 >= r ? b1 - r : b1 + (A - r);  // (B - M) mod A
+    B = W >= b1 ? W - b1 : W + (A - b1);   // reflected
+    M = A;
+    A = r;
+    return false;
+}
+
 template <typename U>
 __device__ __forceinline__ U modsearch_value(U A, U B, U M, U W) {
     uint32_t flips = 0;
     U u;
-    while (true) {
-        if (B <= W) {
-            u = B;
-            break;
-        }
-        const DivBy<U> by(A);
-        if (W + 1 >= A) {
-            const U t = by.rem(M - B);
-            u = t ? A - t : 0;
-            break;
-        }
-        const U r = by.rem(M);
-        U b1 = by.rem(B);
-        b1 = b1 >= r ? b1 - r : b1 + (A - r);  // (B - M) mod A
-        B = W >= b1 ? W - b1 : W + (A - b1);   // reflected
-        M = A;
-        A = r;
+    while (!modsearch_level<U>(A, B, M, W, u)) flips ^= 1u;
+    return flips ? W - u : u;
+}
+
+// Primes above 2^32: the values shrink by a factor ~3 per level, so after one
+// or two levels of 64-bit arithmetic (a double-precision reciprocal per
+// level) the rest runs on 32-bit values.  The levels below keep the
+// invariants (0 < A < M, B < M, W < M - 1), so the 32-bit search continues
+// the same recursion.
+template <>
+__device__ __forceinline__ uint64_t modsearch_value<uint64_t>(uint64_t A, uint64_t B, uint64_t M, uint64_t W) {
+    uint32_t flips = 0;
+    uint64_t u;
+    while (M >> 32) {
+        if (modsearch_level<uint64_t>(A, B, M, W, u)) return flips ? W - u : u;
         flips ^= 1u;
     }
+    u = modsearch_value<uint32_t>((uint32_t)A, (uint32_t)B, (uint32_t)M, (uint32_t)W);
     return flips ? W - u : u;
 }
 

@@ -17,8 +17,10 @@
 //      full (coprime m, windows, list space).  Windows of different requests
 //      (different K, sl, rounds) share the launch; the kernels read each
 //      side's constants from its window's WinInfo.
-//   3. finish the oldest launch in flight and scatter its gaps to the
-//      requests; a request is done when its last window is.
+//   3. finish the oldest launch in flight whose stream is idle: queue its
+//      next continuation or confirmation round if it needs one (it stays in
+//      flight), else scatter its gaps to the requests; a request is done
+//      when its last window is.
 // Two slots (pg_server_params.slots) keep one launch queued behind the running
 // one, so the host work of step 2 overlaps the device; the worker polls the
 // running launch's stream so requests that arrive meanwhile go into a free
@@ -33,8 +35,9 @@
 // host memory the warps read between test rounds); its warps leave after the
 // tests in hand, finalize skips the launch, and the slot keeps the search's
 // device state (SUSPENDED).  A suspended launch resumes from its queue head
-// (the same kernel, same arguments) when fewer than slots - 1 launches run
-// and no cheaper work runs or waits.  A request that has waited
+// (the same kernel, same arguments) when fewer than min(slots - 1, 2)
+// launches run and no cheaper work runs or waits; the slots beyond those hold
+// stopped launches (default 4: two running, one stopped per class overtaken).  A request that has waited
 // max(2 s, 100 x preempt_us) is placed first whatever its class.
 #include <algorithm>
 #include <chrono>
@@ -109,6 +112,7 @@ struct SlotState {
     bool stopping = false;   // its stop flag is raised
     bool suspended = false;  // its search stopped with items queued: resumed later
     double t_run = 0;        // when the launch (or its resume) was enqueued
+    double t_wait = 0;       // submit time of the oldest request with windows in the launch
     uint64_t seq = 0;
 };
 
@@ -346,6 +350,7 @@ struct pg_server {
         ss.tabs.clear();
         const uint32_t layout = next_layout();
         if (!layout) return false;
+        ss.t_wait = now();
         std::vector<std::pair<uint64_t, std::pair<int, std::string>>> failed;
         for (uint64_t id : order) {
             Request &r = reqs.at(id);
@@ -372,6 +377,7 @@ struct pg_server {
                 r.next_m += inc;
                 r.windows++;
                 if (r.t_start < 0) r.t_start = now();
+                ss.t_wait = std::min(ss.t_wait, r.t_submit);
             }
             if (full) break;
         }
@@ -460,7 +466,7 @@ struct pg_server {
         bool idle = false;
         for (const auto &ss : slot) {
             idle |= !ss.inflight && !ss.suspended;
-            if (ss.inflight && !ss.stopping && t - ss.t_run >= limit) c = std::min(c, cls(ss.s.L));
+            if (ss.inflight && !ss.stopping && t - ss.t_wait >= limit) c = std::min(c, cls(ss.s.L));
         }
         double since = -1;
         const uint32_t L = next_layout(&since);
@@ -498,7 +504,9 @@ struct pg_server {
         cudaSetDevice(ctx->device);
         std::unique_lock<std::mutex> lk(mu);
         double busy_since = -1;
-        const size_t run_limit = prm.preempt_us ? slot.size() - 1 : slot.size();
+        // with preemption the slots beyond two hold stopped launches: one per
+        // operand class that was overtaken, and one is kept free
+        const size_t run_limit = prm.preempt_us ? std::min<size_t>(slot.size() - 1, 2) : slot.size();
         while (true) {
             if (!stop) admit(lk);
             // resume stopped launches, oldest first, while there is room
@@ -550,9 +558,13 @@ struct pg_server {
             }
             if (ready) {
                 lk.unlock();
-                const int rc = slot_finish(ready->s);
+                // one step: a launch needing a continuation or confirmation
+                // round gets it queued and stays in flight, so the worker
+                // never waits on the device here
+                const int rc = slot_finish(ready->s, false);
                 const std::string err = rc < 0 ? pg_last_error() : "";
                 lk.lock();
+                if (rc == SLOT_PENDING) continue;
                 ready->inflight = false;
                 ready->stopping = false;
                 if (rc == SLOT_STOPPED) {
@@ -604,7 +616,7 @@ extern "C" int pg_server_create(int device, const pg_server_params *params, pg_s
     if (!p.ext_window) p.ext_window = 64;
     if (p.max_windows > 65535) return fail(PG_ERR_ARG, "max_windows=%u > 65535", p.max_windows);
     if (p.max_sl / 2 > 65535) return fail(PG_ERR_ARG, "max_sl=%u > 131071", p.max_sl);
-    if (!p.slots) p.slots = p.preempt_us ? 3 : 2;
+    if (!p.slots) p.slots = p.preempt_us ? 4 : 2;
     if (p.slots > 8) return fail(PG_ERR_ARG, "slots=%u > 8", p.slots);
     if (p.preempt_us && p.slots < 2) return fail(PG_ERR_ARG, "preemption needs at least 2 slots");
     pg_ctx *c = nullptr;
