@@ -521,7 +521,9 @@ def run_ours(args, rank: int, world: int, local_rank: int, dist) -> dict | None:
         line["configs"]["prp_rates"] = prp_rates(pg, ctx)
         ctx.close()
         line["configs"]["serving"] = run_serve(args, n_jobs=64, compact=True, preempt=0)
-        line["configs"]["serving_preempt"] = run_serve(args, n_jobs=64, compact=True, preempt=SERVE_PREEMPT_US)
+        line["configs"]["serving_preempt"] = run_serve(args, n_jobs=64, compact=True, preempt=SERVE_PREEMPT_US,
+                                                       rate=line["configs"]["serving"]["arrival_rate_jobs_per_s"])
+        line["configs"]["serving_preempt"]["arrival_rate_source"] = "the rate of configs.serving (same load)"
     else:
         ctx.close()
     if world == 1 and not args.no_cpu:
@@ -590,12 +592,14 @@ def serve_requests(n: int = 256, seed: int = SERVE_SEED, limit: int = 1_000_000_
     return out
 
 
-def run_serve(args, n_jobs: int | None = None, compact: bool = False, preempt: int | None = None) -> dict:
+def run_serve(args, n_jobs: int | None = None, compact: bool = False, preempt: int | None = None,
+              rate: float | None = None) -> dict:
     """Capacity (all requests queued at once) and latency under Poisson
     arrivals at 70% of that capacity, through pg_server_*.  compact: the
     short run of the default bench line (n_jobs requests, the server's
     default launch shape); preempt: the server's preempt_us (None = the
-    --serve-preempt-us option)."""
+    --serve-preempt-us option); rate: the arrival rate to use instead (so
+    two servers are compared at one load)."""
     import threading
     import numpy as np
     import __graft_entry__
@@ -623,7 +627,8 @@ def run_serve(args, n_jobs: int | None = None, compact: bool = False, preempt: i
         cap_jobs = len(reqs) / span
         st_closed = srv.stats()
         # open loop: Poisson arrivals at 70% of capacity (or at the given rate)
-        rate = args.serve_rate if args.serve_rate > 0 else 0.7 * cap_jobs
+        rate_source = "the given rate" if rate else ("--serve-rate" if args.serve_rate > 0 else "70% of capacity")
+        rate = rate or (args.serve_rate if args.serve_rate > 0 else 0.7 * cap_jobs)
         gaps = np.random.default_rng(SERVE_SEED + 1).exponential(1.0 / rate, len(reqs))
         arrivals = np.cumsum(gaps)
         ids2 = [None] * len(reqs)
@@ -651,7 +656,8 @@ def run_serve(args, n_jobs: int | None = None, compact: bool = False, preempt: i
                             "placed_p50_ms": round(float(np.percentile(wait[sel], 50)), 1),
                             "placed_p99_ms": round(float(np.percentile(wait[sel], 99)), 1)}
     return {
-        "metric": f"serving latency p99 ({len(reqs)} gap-search requests, Poisson arrivals at 70% of capacity)",
+        "metric": f"serving latency p99 ({len(reqs)} gap-search requests, Poisson arrivals at {rate:.1f}/s)",
+        "arrival_rate_source": rate_source,
         "value": round(float(np.percentile(lat, 99)), 2), "unit": "ms", "higher_is_better": False,
         "p50_ms": round(float(np.percentile(lat, 50)), 2), "p99_ms": round(float(np.percentile(lat, 99)), 2),
         "mean_ms": round(float(lat.mean()), 2), "latency_by_P": by_p,
