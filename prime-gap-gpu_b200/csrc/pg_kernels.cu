@@ -356,6 +356,39 @@ struct DivBy<uint64_t> {
     }
 };
 
+// x mod A for 32-bit x and a divisor A >= 2^13, with one single-precision
+// reciprocal shared by every x.  Each step rounds toward zero (A up, x and
+// the products down) and the reciprocal is scaled by 1 - 2^-20, so the
+// quotient estimate never exceeds floor(x / A); the relative shortfall is
+// below 2^-19.3 (rcp.approx is within one ulp, each rounding within one
+// ulp), so with x / A < 2^19 it falls short by at most one.  The remainder
+// x - q*A then lies in [0, 2A) and is at most x, so it is exact in 32 bits
+// and one conditional subtraction finishes it.
+struct DivByF32 {
+    uint32_t A;
+    float inv;
+    __device__ __forceinline__ explicit DivByF32(uint32_t a) : A(a) {
+        float af, r;
+        asm("cvt.rp.f32.u32 %0, %1;" : "=f"(af) : "r"(a));
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(af));
+        asm("mul.rm.ftz.f32 %0, %1, %2;" : "=f"(inv) : "f"(r), "f"(1.0f - 0x1p-20f));
+    }
+    __device__ __forceinline__ uint32_t rem(uint32_t x) const {
+        float xf, e;
+        uint32_t q;
+        asm("cvt.rm.f32.u32 %0, %1;" : "=f"(xf) : "r"(x));
+        asm("mul.rm.ftz.f32 %0, %1, %2;" : "=f"(e) : "f"(xf), "f"(inv));
+        asm("cvt.rzi.u32.f32 %0, %1;" : "=r"(q) : "f"(e));
+        const uint32_t r = x - q * A;
+        return r >= A ? r - A : r;
+    }
+};
+
+// Windows at least this wide (W = 2*sly) let the 32-bit levels of the
+// modular search use DivByF32: every level that does not end has A > W + 1
+// (and A > W for the walk search over W - 1).
+constexpr uint32_t F32_MIN_W = 1u << 13;
+
 // For 0 < A < M, B < M, W < M - 1 and gcd(A, M) = 1, the value
 // u = (A*x + B) mod M at the smallest x >= 0 with (A*x + B) mod M <= W.
 // If B <= W, x = 0 and u = B.  If W + 1 >= A the first wrap already lands in
@@ -369,20 +402,30 @@ struct DivBy<uint64_t> {
 //
 // One level: true with u set when the search ends here, else the next
 // level's (A, B, M) in place (the caller flips the reflection parity).
-template <typename U>
+// F (32-bit values, W >= F32_MIN_W only): the remainders of a level that
+// does not end use DivByF32.
+template <typename U, bool F>
 __device__ __forceinline__ bool modsearch_level(U &A, U &B, U &M, U W, U &u) {
     if (B <= W) {
         u = B;
         return true;
     }
-    const DivBy<U> by(A);
     if (W + 1 >= A) {
-        const U t = by.rem(M - B);
+        const U t = DivBy<U>(A).rem(M - B);
         u = t ? A - t : 0;
         return true;
     }
-    const U r = by.rem(M);
-    U b1 = by.rem(B);
+    U r, b1;
+    if constexpr (F) {
+        static_assert(sizeof(U) == 4, "DivByF32 takes 32-bit values");
+        const DivByF32 by(A);
+        r = by.rem(M);
+        b1 = by.rem(B);
+    } else {
+        const DivBy<U> by(A);
+        r = by.rem(M);
+        b1 = by.rem(B);
+    }
     b1 = b1 >= r ? b1 - r : b1 + (A - r);  // (B - M) mod A
     B = W >= b1 ? W - b1 : W + (A - b1);   // reflected
     M = A;
@@ -390,29 +433,61 @@ __device__ __forceinline__ bool modsearch_level(U &A, U &B, U &M, U W, U &u) {
     return false;
 }
 
-template <typename U>
-__device__ __forceinline__ U modsearch_value(U A, U B, U M, U W) {
-    uint32_t flips = 0;
-    U u;
-    while (!modsearch_level<U>(A, B, M, W, u)) flips ^= 1u;
-    return flips ? W - u : u;
+// M * J <= M0 without overflow (M < 2^40, J < 2^32).
+__device__ __forceinline__ bool prod_le(uint32_t M, uint64_t J, uint32_t M0) { return (uint64_t)M * J <= M0; }
+__device__ __forceinline__ bool prod_le(uint64_t M, uint64_t J, uint64_t M0) {
+    return __umul64hi(M, J) == 0 && M * J <= M0;
 }
 
-// Primes above 2^32: the values shrink by a factor ~3 per level, so after one
-// or two levels of 64-bit arithmetic (a double-precision reciprocal per
-// level) the rest runs on 32-bit values.  The levels below keep the
-// invariants (0 < A < M, B < M, W < M - 1), so the 32-bit search continues
-// the same recursion.
-template <>
-__device__ __forceinline__ uint64_t modsearch_value<uint64_t>(uint64_t A, uint64_t B, uint64_t M, uint64_t W) {
+// The search restricted to x < J (E set): false when the first hit lies at
+// x >= J.  Bound: a level whose value B is above W has no hit at x = 0, so
+// its own x_k >= 1; the level above it lands its hit at
+// x = ceil(((x_k + 1) * M - B) / A) > x_k * M / A, and M of the level below
+// is that A, so over the levels x_0 >= x_k * M_0 / M_k.  Once
+// M_k * J <= M_0 with B_k > W, x_0 >= J and the levels between M_0 / J and
+// about W are skipped.  A lane that stops early only pays off when its whole
+// warp does, so callers set E where a prime expects well under one hit.
+// Values of 64 bits run their levels in 32-bit arithmetic once they fit.
+template <typename U, bool F, bool E>
+__device__ __forceinline__ bool modsearch_within(U A, U B, U M, U W, uint64_t J, U &u_out) {
+    const U M0 = M;
     uint32_t flips = 0;
-    uint64_t u;
-    while (M >> 32) {
-        if (modsearch_level<uint64_t>(A, B, M, W, u)) return flips ? W - u : u;
-        flips ^= 1u;
+    U u;
+    if constexpr (sizeof(U) == 8) {
+        while (M >> 32) {
+            if (E && B > W && prod_le(M, J, M0)) return false;
+            if (modsearch_level<uint64_t, false>(A, B, M, W, u)) {
+                u_out = flips ? W - u : u;
+                return true;
+            }
+            flips ^= 1u;
+        }
+        uint32_t A32 = (uint32_t)A, B32 = (uint32_t)B, M32 = (uint32_t)M, u32;
+        const uint32_t W32 = (uint32_t)W;
+        while (true) {  // M32 * J < 2^64: J < 2^32
+            if (E && B32 > W32 && (uint64_t)M32 * J <= M0) return false;
+            if (modsearch_level<uint32_t, F>(A32, B32, M32, W32, u32)) break;
+            flips ^= 1u;
+        }
+        u_out = flips ? W - u32 : u32;
+        return true;
+    } else {
+        while (true) {
+            if (E && B > W && prod_le(M, J, M0)) return false;
+            if (modsearch_level<U, F>(A, B, M, W, u)) break;
+            flips ^= 1u;
+        }
+        u_out = flips ? W - u : u;
+        return true;
     }
-    u = modsearch_value<uint32_t>((uint32_t)A, (uint32_t)B, (uint32_t)M, (uint32_t)W);
-    return flips ? W - u : u;
+}
+
+// The search without a bound on x.
+template <typename U, bool F = false>
+__device__ __forceinline__ U modsearch_value(U A, U B, U M, U W) {
+    U u;
+    modsearch_within<U, F, false>(A, B, M, W, 0, u);
+    return u;
 }
 
 // Arithmetic mod a prime p < 2^32 with a double-precision reciprocal: the
@@ -476,8 +551,10 @@ struct Mod40 {
 //
 // With the job's walk steps (wk != NULL: sa, sb precomputed, alpha and beta
 // two modular products away) every hit after the first is one walk step,
-// whatever the number of hits.
-template <typename U, typename Mod>
+// whatever the number of hits.  F: 32-bit search levels with DivByF32
+// (W >= F32_MIN_W); E: searches stop once their hit provably lies past the
+// window.
+template <typename U, typename Mod, bool F, bool E>
 __device__ __forceinline__ void sieve_prime(const LargeArgs &a, const uint32_t *s_wheel, const Mod &md, U c, U ci,
                                             const WalkC *wk) {
     const U p = md.p;
@@ -489,7 +566,8 @@ __device__ __forceinline__ void sieve_prime(const LargeArgs &a, const uint32_t *
     const U Ainv = p - ci; // (-K)^-1
     uint64_t j = 0;
     while (true) {
-        const U u = modsearch_value<U>(A, B, p, W);
+        U u;
+        if (!modsearch_within<U, F, E>(A, B, p, W, a.nodd - j, u)) return;
         j += md.mul(md.sub(u, B), Ainv);
         if (j >= a.nodd) return;
         mark_hit(a, s_wheel, j, (uint32_t)u);
@@ -502,10 +580,10 @@ __device__ __forceinline__ void sieve_prime(const LargeArgs &a, const uint32_t *
                 alpha = md.mul(A, (U)sa);
                 beta = p - md.mul(A, (U)sb);
             } else {
-                alpha = modsearch_value<U>(A, A, p, W);
+                alpha = modsearch_value<U, F>(A, A, p, W);
                 sa = 1 + (uint64_t)md.mul(md.sub(alpha, A), Ainv);
                 const U aw = A + W >= p ? A + W - p : A + W;
-                const U ub = modsearch_value<U>(A, aw, p, W - 1);
+                const U ub = modsearch_value<U, F>(A, aw, p, W - 1);
                 beta = W - ub;
                 sb = 1 + (uint64_t)md.mul(md.sub(ub, aw), Ainv);
             }
@@ -531,25 +609,39 @@ __device__ __forceinline__ void sieve_prime(const LargeArgs &a, const uint32_t *
 }
 
 // One thread per prime of [first, first + count); the block keeps the wheel
-// row in shared memory.
-template <typename T>
+// row in shared memory.  A warp whose 32 primes all expect under 1/64 hit in
+// the window (p > 64 * nodd * (W + 1)) bounds its searches by the window
+// (modsearch_within): it then skips their last levels with odds of at least
+// one half; a lane alone cannot, as its warp runs as long as its deepest lane.
+template <typename T, bool F>
 __global__ void __launch_bounds__(256) k_sieve_large_search(const __grid_constant__ LargeArgs a, uint64_t first,
                                                             uint64_t count) {
     extern __shared__ uint32_t s_wheel[];
     for (uint32_t w = threadIdx.x; w < a.words; w += blockDim.x) s_wheel[w] = a.wheel[w];
     __syncthreads();
     const uint64_t i = first + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= first + count) return;
-    const uint64_t p = ((const T *)a.p)[i];
+    const bool valid = i < first + count;
+    const uint64_t p = valid ? (uint64_t)((const T *)a.p)[i] : 0;
+    const bool sparse = __all_sync(0xffffffffu, !valid || a.nodd * (2ull * a.sly + 1) * 64 < p);
+    if (!valid) return;
     const uint64_t c = ((const T *)a.c)[i];
     const uint64_t ci = ((const T *)a.cinv)[i];
     const bool walk = a.walk && i >= a.walk_first && i < a.walk_end;  // walk steps are kept below 2^32 only
     WalkC wk;
     if (walk) wk = a.walk[i - a.walk_first];
-    if (p < (1ull << 32))
-        sieve_prime<uint32_t, Mod32>(a, s_wheel, Mod32((uint32_t)p), (uint32_t)c, (uint32_t)ci, walk ? &wk : nullptr);
-    else
-        sieve_prime<uint64_t, Mod40>(a, s_wheel, Mod40(p), c, ci, nullptr);
+    if (p < (1ull << 32)) {
+        const Mod32 md((uint32_t)p);
+        if (sparse)
+            sieve_prime<uint32_t, Mod32, F, true>(a, s_wheel, md, (uint32_t)c, (uint32_t)ci, walk ? &wk : nullptr);
+        else
+            sieve_prime<uint32_t, Mod32, F, false>(a, s_wheel, md, (uint32_t)c, (uint32_t)ci, walk ? &wk : nullptr);
+    } else {
+        const Mod40 md(p);
+        if (sparse)
+            sieve_prime<uint64_t, Mod40, F, true>(a, s_wheel, md, c, ci, nullptr);
+        else
+            sieve_prime<uint64_t, Mod40, F, false>(a, s_wheel, md, c, ci, nullptr);
+    }
 }
 
 // Walk constants (alpha, sa, beta, sb of sieve_prime) of the primes
@@ -611,7 +703,8 @@ __global__ void __launch_bounds__(256) k_sieve_large_seg(const __grid_constant__
     const uint32_t alpha = md.mul(A, wk.sa), beta = p - md.mul(A, wk.sb);
     const uint32_t B0 = md.sub(a.sly % p, md.mul(md.red(a.m0), c2));
     const uint32_t B = md.red((uint64_t)md.mul(A, md.red(j0)) + B0);  // residue at j0
-    const uint32_t u = modsearch_value<uint32_t>(A, B, p, W);
+    const uint32_t u = W >= F32_MIN_W ? modsearch_value<uint32_t, true>(A, B, p, W)
+                                      : modsearch_value<uint32_t, false>(A, B, p, W);
     uint64_t j = j0 + md.mul(md.sub(u, B), Ainv);
     if (j >= j1) return;
     mark_hit(a, s_wheel, j, u);
@@ -664,10 +757,15 @@ cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, co
     if (search_first < a.np) {  // the rest: modular search for each hit
         const uint64_t count = a.np - search_first;
         const uint64_t blocks = (count + threads - 1) / threads;
-        if (wide)
-            k_sieve_large_search<uint64_t><<<(unsigned)blocks, threads, smem, st>>>(a, search_first, count);
+        const bool f32 = 2ull * a.sly >= F32_MIN_W;  // every 32-bit level that does not end has A >= 2^13
+        if (wide && f32)
+            k_sieve_large_search<uint64_t, true><<<(unsigned)blocks, threads, smem, st>>>(a, search_first, count);
+        else if (wide)
+            k_sieve_large_search<uint64_t, false><<<(unsigned)blocks, threads, smem, st>>>(a, search_first, count);
+        else if (f32)
+            k_sieve_large_search<uint32_t, true><<<(unsigned)blocks, threads, smem, st>>>(a, search_first, count);
         else
-            k_sieve_large_search<uint32_t><<<(unsigned)blocks, threads, smem, st>>>(a, search_first, count);
+            k_sieve_large_search<uint32_t, false><<<(unsigned)blocks, threads, smem, st>>>(a, search_first, count);
     }
     return cudaGetLastError();
 }
