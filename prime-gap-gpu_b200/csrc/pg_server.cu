@@ -711,10 +711,19 @@ extern "C" int pg_server_wait(pg_server *srv, uint64_t id, double timeout_s, uin
                               uint32_t *next_gap, pg_request_info *info) {
     if (!srv) return fail(PG_ERR_ARG, "pg_server_wait: server is NULL");
     std::unique_lock<std::mutex> lk(srv->mu);
-    auto it = srv->reqs.find(id);
-    if (it == srv->reqs.end()) return fail(PG_ERR_ARG, "pg_server_wait: no request %llu", (unsigned long long)id);
-    if (!wait_on(srv->cv_done, lk, timeout_s, [&] { return it->second.state == St::DONE; }))
+    if (srv->reqs.find(id) == srv->reqs.end())
+        return fail(PG_ERR_ARG, "pg_server_wait: no request %llu", (unsigned long long)id);
+    // looked up again after every wake-up: another waiter of the same id may
+    // have returned it (and erased it) meanwhile
+    auto done_or_gone = [&] {
+        auto f = srv->reqs.find(id);
+        return f == srv->reqs.end() || f->second.state == St::DONE;
+    };
+    if (!wait_on(srv->cv_done, lk, timeout_s, done_or_gone))
         return fail(PG_ERR_TIMEOUT, "request %llu not done", (unsigned long long)id);
+    auto it = srv->reqs.find(id);
+    if (it == srv->reqs.end())
+        return fail(PG_ERR_ARG, "pg_server_wait: request %llu was returned to another waiter", (unsigned long long)id);
     Request &r = it->second;
     const size_t n = r.ms.size();
     if (info) {

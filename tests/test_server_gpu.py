@@ -134,6 +134,29 @@ def test_request_errors(pg):
             assert len(srv.wait(big).ms) == pg.count_m(1_000_000, 40_000, 2190)
 
 
+def test_two_waiters_of_one_request(pg):
+    """Two threads wait on the same request id through the C ABI: one receives the gaps, the other a
+    PG_ERR_ARG that says the request went to another waiter; neither reads a request already returned."""
+    with pg.Server(batch_m=2_000, window_m=2_000, max_windows=4, max_sl=4_000) as srv:
+        rid = srv.submit(503, 2190, 3_000, 20_000_000, 1_000_000, 6_000)
+        n = pg.count_m(1_000_000, 6_000, 2190)
+        res = []  # (status, next gaps) per waiter
+
+        def waiter():
+            nxt = np.zeros(n, dtype=np.uint32)
+            p32 = nxt.ctypes.data_as(pg.lib.pg_server_wait.argtypes[5])
+            rc = pg.lib.pg_server_wait(srv._h, rid, 120.0, None, None, p32, None)
+            res.append((rc, nxt))
+
+        th = [threading.Thread(target=waiter) for _ in range(2)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        assert sorted(rc for rc, _ in res) == [-1, 0]
+        assert all((nxt > 0).all() for rc, nxt in res if rc == 0)
+
+
 def test_destroy_fails_queued_requests(pg):
     srv = pg.Server(batch_m=2_000, window_m=1_000, max_windows=2, max_sl=4_000)
     for k in range(6):

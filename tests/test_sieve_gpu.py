@@ -59,6 +59,10 @@ def test_large_prime_methods_agree(pg, oracle, flags, P, d, sl, limit, m_start, 
 @pytest.mark.parametrize("P,d,sl,limit,m_start,m_inc", [
     (503, 2190, 4_000, 4_300_000_000, 1_000_000, 60),
     (211, 2310, 300, 4_400_000_000, 10**12 + 1, 60),    # m above 2^32, short rows
+    # W >= 8192: single-precision quotients on the 32-bit levels; few odd m, so warps of primes
+    # expecting under 1/64 hit stop their searches at the window bound, from the 64-bit levels on
+    (907, 210, 18_000, 4_300_000_000, 1_000_000, 60),
+    (503, 2190, 10_000, 4_300_000_000, 1_000_001, 120),
 ])
 def test_wide_primes_above_2_32(pg, oracle, P, d, sl, limit, m_start, m_inc):
     """max_prime above 2^32: 64-bit prime tables and residues."""
