@@ -659,7 +659,7 @@ static int run_sieve(Slot &s, const WinPart &w, bool compact) {
     int nb = 0;
     const uint64_t search_first = seg_bands(j, split, w.nodd, bands, &nb);
     PG_CUDA(launch_sieve_large(la, T.wide, split, bands, nb, search_first, s.st));
-    s.sst.kernel_launches += (split > 0) + nb + (search_first < T.np);
+    s.sst.kernel_launches += (split > 0) + (nb > 0) + (search_first < T.np);
     SieveArgs sa{};
     sa.sly = j->sly;
     sa.words = j->W;

@@ -682,16 +682,34 @@ cudaError_t launch_walk_consts(const void *p, const void *c, const void *ci, boo
 // (A*j0 + B) mod p; every later hit of the segment from the prime's walk
 // constants.  A prime expecting thousands of hits per window is thus spread
 // over many threads of similar work instead of one long serial walk.
+//
+// Every band of a window (its own segment count) runs in this one launch:
+// block b belongs to the first band whose cumulative block count exceeds b,
+// and inside the band to segment (b' / prime blocks), prime block
+// (b' mod prime blocks).  Bands of a few thousand blocks, each too short to
+// fill the SMs through its tail, so overlap.
+struct SegGrid {
+    SegBand band[MAX_SEG_BANDS];
+    uint32_t block_end[MAX_SEG_BANDS];  // blocks of bands 0 .. b
+    uint32_t pblocks[MAX_SEG_BANDS];    // blocks of 256 primes in band b
+    int nbands;
+};
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_sieve_large_seg(const __grid_constant__ LargeArgs a, uint64_t first,
-                                                         uint64_t count, uint32_t seg_len) {
+__global__ void __launch_bounds__(256) k_sieve_large_seg(const __grid_constant__ LargeArgs a,
+                                                         const __grid_constant__ SegGrid g) {
     extern __shared__ uint32_t s_wheel[];
     for (uint32_t w = threadIdx.x; w < a.words; w += blockDim.x) s_wheel[w] = a.wheel[w];
     __syncthreads();
-    const uint64_t i = first + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t j0 = (uint64_t)blockIdx.y * seg_len;
-    if (i >= first + count || j0 >= a.nodd) return;
-    const uint64_t j1 = min(a.nodd, j0 + seg_len);
+    int b = 0;
+    while (b + 1 < g.nbands && blockIdx.x >= g.block_end[b]) b++;
+    const uint32_t local = blockIdx.x - (b ? g.block_end[b - 1] : 0u);
+    const uint32_t seg = local / g.pblocks[b];
+    const SegBand &bd = g.band[b];
+    const uint64_t i = bd.first + (uint64_t)(local - seg * g.pblocks[b]) * blockDim.x + threadIdx.x;
+    const uint64_t j0 = (uint64_t)seg * bd.seg_len;
+    if (i >= bd.first + bd.count || j0 >= a.nodd) return;
+    const uint64_t j1 = min(a.nodd, j0 + bd.seg_len);
     const uint32_t p = (uint32_t)((const T *)a.p)[i];
     const uint32_t c = (uint32_t)((const T *)a.c)[i];
     const uint32_t ci = (uint32_t)((const T *)a.cinv)[i];
@@ -706,22 +724,31 @@ __global__ void __launch_bounds__(256) k_sieve_large_seg(const __grid_constant__
     const uint32_t u = W >= F32_MIN_W ? modsearch_value<uint32_t, true>(A, B, p, W)
                                       : modsearch_value<uint32_t, false>(A, B, p, W);
     uint64_t j = j0 + md.mul(md.sub(u, B), Ainv);
-    if (j >= j1) return;
-    mark_hit(a, s_wheel, j, u);
     uint32_t v = u;
-    while (true) {
-        if (v + alpha <= W) {
-            j += wk.sa;
-            v += alpha;
-        } else if (v >= beta) {
-            j += wk.sb;
-            v -= beta;
-        } else {
-            j += (uint64_t)wk.sa + wk.sb;
-            v = v + alpha - beta;
+    // The walk, SEG_BATCH hits at a time: the steps (selects, no branches)
+    // come first, then the batch's rank loads are issued together so their
+    // latencies overlap, then its marks; hits at or past j1 are masked.
+    constexpr int SEG_BATCH = 4;
+    while (j < j1) {
+        uint64_t jj[SEG_BATCH];
+        uint32_t vv[SEG_BATCH];
+#pragma unroll
+        for (int k = 0; k < SEG_BATCH; k++) {
+            jj[k] = j;
+            vv[k] = v;
+            const bool up = v + alpha <= W, down = v >= beta;
+            j += up ? wk.sa : (down ? wk.sb : (uint64_t)wk.sa + wk.sb);
+            v = up ? v + alpha : (down ? v - beta : v + alpha - beta);
         }
-        if (j >= j1) return;
-        mark_hit(a, s_wheel, j, v);
+        int32_t r[SEG_BATCH];
+#pragma unroll
+        for (int k = 0; k < SEG_BATCH; k++) {
+            const bool skip = jj[k] >= j1 || ((s_wheel[vv[k] >> 5] >> (vv[k] & 31)) & 1u);
+            r[k] = skip ? -1 : a.rank[jj[k]];
+        }
+#pragma unroll
+        for (int k = 0; k < SEG_BATCH; k++)
+            if (r[k] >= 0) atomicOr(&a.bitmaps[(size_t)r[k] * a.words + (vv[k] >> 5)], 1u << (vv[k] & 31));
     }
 }
 
@@ -731,14 +758,24 @@ cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, co
     const uint32_t threads = 256;
     const size_t smem = (size_t)a.words * sizeof(uint32_t);
     if (split > a.np) split = a.np;
-    for (int b = 0; b < nbands; b++) {
+    SegGrid g{};
+    uint64_t blocks = 0;
+    for (int b = 0; b < nbands && b < MAX_SEG_BANDS; b++) {
         const SegBand &bd = bands[b];
-        if (bd.count == 0) continue;
-        const dim3 grid((unsigned)((bd.count + threads - 1) / threads), bd.nseg);
+        if (bd.count == 0 || bd.nseg == 0) continue;
+        const uint64_t pb = (bd.count + threads - 1) / threads;
+        blocks += pb * bd.nseg;
+        if (blocks >= (1ull << 31)) return cudaErrorInvalidConfiguration;
+        g.band[g.nbands] = bd;
+        g.pblocks[g.nbands] = (uint32_t)pb;
+        g.block_end[g.nbands] = (uint32_t)blocks;
+        g.nbands++;
+    }
+    if (blocks) {
         if (wide)
-            k_sieve_large_seg<uint64_t><<<grid, threads, smem, st>>>(a, bd.first, bd.count, bd.seg_len);
+            k_sieve_large_seg<uint64_t><<<(unsigned)blocks, threads, smem, st>>>(a, g);
         else
-            k_sieve_large_seg<uint32_t><<<grid, threads, smem, st>>>(a, bd.first, bd.count, bd.seg_len);
+            k_sieve_large_seg<uint32_t><<<(unsigned)blocks, threads, smem, st>>>(a, g);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
