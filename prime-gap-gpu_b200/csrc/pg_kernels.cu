@@ -537,6 +537,40 @@ struct Mod40 {
     __device__ __forceinline__ uint64_t sub(uint64_t a, uint64_t b) const { return a >= b ? a - b : a + (p - b); }
 };
 
+// Marks every hit of a prime's walk from the hit (j, v) (inclusive) up to
+// j_end: the hit after v is v + alpha (step sa) if that is <= W, else
+// v - beta (step sb) if v >= beta, else v + alpha - beta (step sa + sb).
+// WALK_BATCH hits at a time: their steps (selects, no branches) come first,
+// then the batch's rank loads are issued together so their latencies
+// overlap, then its marks; hits at or past j_end are masked.
+constexpr int WALK_BATCH = 4;
+
+template <typename U>
+__device__ __forceinline__ void walk_marks(const LargeArgs &a, const uint32_t *s_wheel, uint64_t j, U v,
+                                           uint64_t j_end, U alpha, U beta, U W, uint64_t sa, uint64_t sb) {
+    while (j < j_end) {
+        uint64_t jj[WALK_BATCH];
+        uint32_t vv[WALK_BATCH];
+#pragma unroll
+        for (int k = 0; k < WALK_BATCH; k++) {
+            jj[k] = j;
+            vv[k] = (uint32_t)v;
+            const bool up = v + alpha <= W, down = v >= beta;
+            j += up ? sa : (down ? sb : sa + sb);
+            v = up ? v + alpha : (down ? v - beta : v + alpha - beta);
+        }
+        int32_t r[WALK_BATCH];
+#pragma unroll
+        for (int k = 0; k < WALK_BATCH; k++) {
+            const bool skip = jj[k] >= j_end || ((s_wheel[vv[k] >> 5] >> (vv[k] & 31)) & 1u);
+            r[k] = skip ? -1 : a.rank[jj[k]];
+        }
+#pragma unroll
+        for (int k = 0; k < WALK_BATCH; k++)
+            if (r[k] >= 0) atomicOr(&a.bitmaps[(size_t)r[k] * a.words + (vv[k] >> 5)], 1u << (vv[k] & 31));
+    }
+}
+
 // Sieve of one prime p > 2*sly + 1 over the window.  With X = 2Y and the
 // odd m = m0 + 2j, p | m*K + X  <=>  u = Y + sly = (A*j + B) mod p with
 // A = -K mod p and B = sly - m0*K/2 mod p; every j of the window with
@@ -570,7 +604,6 @@ __device__ __forceinline__ void sieve_prime(const LargeArgs &a, const uint32_t *
         if (!modsearch_within<U, F, E>(A, B, p, W, a.nodd - j, u)) return;
         j += md.mul(md.sub(u, B), Ainv);
         if (j >= a.nodd) return;
-        mark_hit(a, s_wheel, j, (uint32_t)u);
         if (wk || (a.nodd - j - 1) * (uint64_t)(W + 1) >= 2ull * p) {  // steps known, or 2+ hits expected: walk
             U alpha, beta;
             uint64_t sa, sb;
@@ -587,22 +620,10 @@ __device__ __forceinline__ void sieve_prime(const LargeArgs &a, const uint32_t *
                 beta = W - ub;
                 sb = 1 + (uint64_t)md.mul(md.sub(ub, aw), Ainv);
             }
-            U v = u;
-            while (true) {
-                if (v + alpha <= W) {
-                    j += sa;
-                    v += alpha;
-                } else if (v >= beta) {
-                    j += sb;
-                    v -= beta;
-                } else {
-                    j += sa + sb;
-                    v = v + alpha - beta;
-                }
-                if (j >= a.nodd) return;
-                mark_hit(a, s_wheel, j, (uint32_t)v);
-            }
+            walk_marks<U>(a, s_wheel, j, u, a.nodd, alpha, beta, W, sa, sb);
+            return;
         }
+        mark_hit(a, s_wheel, j, (uint32_t)u);
         B = u + A >= p ? u + A - p : u + A;  // residue of j + 1
         j++;
     }
@@ -723,33 +744,7 @@ __global__ void __launch_bounds__(256) k_sieve_large_seg(const __grid_constant__
     const uint32_t B = md.red((uint64_t)md.mul(A, md.red(j0)) + B0);  // residue at j0
     const uint32_t u = W >= F32_MIN_W ? modsearch_value<uint32_t, true>(A, B, p, W)
                                       : modsearch_value<uint32_t, false>(A, B, p, W);
-    uint64_t j = j0 + md.mul(md.sub(u, B), Ainv);
-    uint32_t v = u;
-    // The walk, SEG_BATCH hits at a time: the steps (selects, no branches)
-    // come first, then the batch's rank loads are issued together so their
-    // latencies overlap, then its marks; hits at or past j1 are masked.
-    constexpr int SEG_BATCH = 4;
-    while (j < j1) {
-        uint64_t jj[SEG_BATCH];
-        uint32_t vv[SEG_BATCH];
-#pragma unroll
-        for (int k = 0; k < SEG_BATCH; k++) {
-            jj[k] = j;
-            vv[k] = v;
-            const bool up = v + alpha <= W, down = v >= beta;
-            j += up ? wk.sa : (down ? wk.sb : (uint64_t)wk.sa + wk.sb);
-            v = up ? v + alpha : (down ? v - beta : v + alpha - beta);
-        }
-        int32_t r[SEG_BATCH];
-#pragma unroll
-        for (int k = 0; k < SEG_BATCH; k++) {
-            const bool skip = jj[k] >= j1 || ((s_wheel[vv[k] >> 5] >> (vv[k] & 31)) & 1u);
-            r[k] = skip ? -1 : a.rank[jj[k]];
-        }
-#pragma unroll
-        for (int k = 0; k < SEG_BATCH; k++)
-            if (r[k] >= 0) atomicOr(&a.bitmaps[(size_t)r[k] * a.words + (vv[k] >> 5)], 1u << (vv[k] & 31));
-    }
+    walk_marks<uint32_t>(a, s_wheel, j0 + md.mul(md.sub(u, B), Ainv), u, j1, alpha, beta, W, wk.sa, wk.sb);
 }
 
 cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, const SegBand *bands, int nbands,
