@@ -603,8 +603,8 @@ static uint64_t large_split(const pg_job *j, uint64_t nodd) {
 // of one segment lie within 2^19 of each other), each cut into the power of
 // two of segments that leaves about SEG_HITS expected hits per (prime,
 // segment) item at the segment's smallest prime; neighbouring segments with
-// the same count share a launch.  Returns the first prime index left to the
-// one-thread-per-prime kernel.
+// the same count share a band (all bands of a window run in one launch).
+// Returns the first prime index left to the one-thread-per-prime kernel.
 static uint64_t seg_bands(const pg_job *j, uint64_t split, uint64_t nodd, SegBand *bands, int *nb) {
     *nb = 0;
     const pg::Tables &T = *j->T;

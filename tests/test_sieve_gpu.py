@@ -145,3 +145,19 @@ def test_segmented_large_prime_rows(pg, oracle, P, d, sl, limit, small, m_start,
             ms, rows = job.sieve_interval(start, inc)
             sel = np.arange(0, len(ms), 53)
             assert np.array_equal(rows[sel], oj.sieve_m(ms[sel]))
+
+
+@pytest.mark.parametrize("P,d,sl,limit,small,m_start,m_inc", [
+    (503, 2190, 30_000, 60_000_000, 0, 1_000_000, 24),          # bound from p > 64 * 12 * 30 001 = 2.3e7
+    (337, 2310, 9_000, 200_000_000, 0, 10_000_000, 40),         # W = 9 000: single-precision quotients
+    (151, 2310, 20_000, 100_000_000, 2_000, 10**12 + 1, 16),    # m above 2^32
+])
+def test_bounded_search_rows(pg, oracle, P, d, sl, limit, small, m_start, m_inc):
+    """Windows of a few odd m and wide rows: warps whose primes all expect under 1/64 hit stop each
+    modular search once it provably lands past the window, and the 32-bit levels take their quotients from
+    a rounded-down single-precision reciprocal (W >= 8192); every row equals the oracle's."""
+    with _job(pg, P, d, sl, limit, m_start, m_inc, small_limit=small) as job:
+        ms, rows = job.sieve_interval(m_start, m_inc)
+    with oracle.Job(P, d, sl, limit) as oj:
+        want = oj.sieve_m(ms)
+    assert len(ms) > 0 and np.array_equal(rows, want)
