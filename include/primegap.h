@@ -380,7 +380,8 @@ int pg_server_submit(pg_server *srv, const pg_request *rq, uint64_t *id);
 /* Waits up to timeout_s seconds (< 0 = for ever) for request id, then copies
  * its results (arrays of info->m_count = pg_count_m(...) entries, ascending
  * m; any may be NULL) and forgets the request.  PG_ERR_TIMEOUT if it is not
- * done yet (it stays queued); the request's own error if it failed. */
+ * done yet (it stays queued); the request's own error if it failed;
+ * PG_ERR_ARG for an unknown id or one another waiter has already returned. */
 int pg_server_wait(pg_server *srv, uint64_t id, double timeout_s, uint64_t *ms, uint32_t *prev_gap,
                    uint32_t *next_gap, pg_request_info *info);
 /* Id of a finished request not yet returned by this call, oldest first;
