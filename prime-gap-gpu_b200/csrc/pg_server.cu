@@ -624,7 +624,11 @@ extern "C" int pg_server_create(int device, const pg_server_params *params, pg_s
     if (rc) return rc;
     if (!p.hbm_budget) {
         size_t free_b = 0, total_b = 0;
-        cudaMemGetInfo(&free_b, &total_b);
+        const cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
+        if (e != cudaSuccess) {
+            pg_ctx_destroy(c);
+            return fail(PG_ERR_CUDA, "pg_server_create: cudaMemGetInfo: %s", cudaGetErrorString(e));
+        }
         p.hbm_budget = free_b / 4 * 3;
     }
     pg_server *srv = new pg_server();
