@@ -542,14 +542,16 @@ struct Mod40 {
 // v - beta (step sb) if v >= beta, else v + alpha - beta (step sa + sb).
 // WALK_BATCH hits at a time: their steps (selects, no branches) come first,
 // then the batch's rank loads are issued together so their latencies
-// overlap, then its marks; hits at or past j_end are masked.
+// overlap, then its marks; hits at or past j_end are masked.  The walk is
+// bound by the integer ALU pipe, so walk_from counts j in 32 bits whenever
+// j_end + sa + sb < 2^32 (no step from j < j_end can then wrap).
 constexpr int WALK_BATCH = 4;
 
-template <typename U>
-__device__ __forceinline__ void walk_marks(const LargeArgs &a, const uint32_t *s_wheel, uint64_t j, U v,
-                                           uint64_t j_end, U alpha, U beta, U W, uint64_t sa, uint64_t sb) {
+template <typename U, typename J>
+__device__ __forceinline__ void walk_marks(const LargeArgs &a, const uint32_t *s_wheel, J j, U v, J j_end, U alpha,
+                                           U beta, U W, J sa, J sb) {
     while (j < j_end) {
-        uint64_t jj[WALK_BATCH];
+        J jj[WALK_BATCH];
         uint32_t vv[WALK_BATCH];
 #pragma unroll
         for (int k = 0; k < WALK_BATCH; k++) {
@@ -569,6 +571,17 @@ __device__ __forceinline__ void walk_marks(const LargeArgs &a, const uint32_t *s
         for (int k = 0; k < WALK_BATCH; k++)
             if (r[k] >= 0) atomicOr(&a.bitmaps[(size_t)r[k] * a.words + (vv[k] >> 5)], 1u << (vv[k] & 31));
     }
+}
+
+template <typename U>
+__device__ __forceinline__ void walk_from(const LargeArgs &a, const uint32_t *s_wheel, uint64_t j, U v,
+                                          uint64_t j_end, U alpha, U beta, U W, uint64_t sa, uint64_t sb) {
+    if (j >= j_end) return;
+    if (j_end + sa + sb < (1ull << 32))
+        walk_marks<U, uint32_t>(a, s_wheel, (uint32_t)j, v, (uint32_t)j_end, alpha, beta, W, (uint32_t)sa,
+                                (uint32_t)sb);
+    else
+        walk_marks<U, uint64_t>(a, s_wheel, j, v, j_end, alpha, beta, W, sa, sb);
 }
 
 // Sieve of one prime p > 2*sly + 1 over the window.  With X = 2Y and the
@@ -620,7 +633,7 @@ __device__ __forceinline__ void sieve_prime(const LargeArgs &a, const uint32_t *
                 beta = W - ub;
                 sb = 1 + (uint64_t)md.mul(md.sub(ub, aw), Ainv);
             }
-            walk_marks<U>(a, s_wheel, j, u, a.nodd, alpha, beta, W, sa, sb);
+            walk_from<U>(a, s_wheel, j, u, a.nodd, alpha, beta, W, sa, sb);
             return;
         }
         mark_hit(a, s_wheel, j, (uint32_t)u);
@@ -744,7 +757,7 @@ __global__ void __launch_bounds__(256) k_sieve_large_seg(const __grid_constant__
     const uint32_t B = md.red((uint64_t)md.mul(A, md.red(j0)) + B0);  // residue at j0
     const uint32_t u = W >= F32_MIN_W ? modsearch_value<uint32_t, true>(A, B, p, W)
                                       : modsearch_value<uint32_t, false>(A, B, p, W);
-    walk_marks<uint32_t>(a, s_wheel, j0 + md.mul(md.sub(u, B), Ainv), u, j1, alpha, beta, W, wk.sa, wk.sb);
+    walk_from<uint32_t>(a, s_wheel, j0 + md.mul(md.sub(u, B), Ainv), u, j1, alpha, beta, W, wk.sa, wk.sb);
 }
 
 cudaError_t launch_sieve_large(const LargeArgs &a, bool wide, uint64_t split, const SegBand *bands, int nbands,
