@@ -443,11 +443,13 @@ __device__ __forceinline__ bool prod_le(uint64_t M, uint64_t J, uint64_t M0) {
 // x >= J.  Bound: a level whose value B is above W has no hit at x = 0, so
 // its own x_k >= 1; the level above it lands its hit at
 // x = ceil(((x_k + 1) * M - B) / A) > x_k * M / A, and M of the level below
-// is that A, so over the levels x_0 >= x_k * M_0 / M_k.  Once
-// M_k * J <= M_0 with B_k > W, x_0 >= J and the levels between M_0 / J and
-// about W are skipped.  A lane that stops early only pays off when its whole
-// warp does, so callers set E where a prime expects well under one hit.
-// Values of 64 bits run their levels in 32-bit arithmetic once they fit.
+// is that A, so over the levels x_0 >= x_k * M_0 / M_k.  So at the first
+// level with M_k * J <= M_0 the search ends: with B_k > W its hit lies at
+// x_0 >= J, otherwise B_k <= W is the hit; the levels between M_0 / J and
+// about W are skipped.  The test costs a product and a compare per level,
+// so callers set E only where it saves many levels (primes expecting well
+// under one hit).  Values of 64 bits run their levels in 32-bit arithmetic
+// once they fit.
 template <typename U, bool F, bool E>
 __device__ __forceinline__ bool modsearch_within(U A, U B, U M, U W, uint64_t J, U &u_out) {
     const U M0 = M;
@@ -645,8 +647,10 @@ __device__ __forceinline__ void sieve_prime(const LargeArgs &a, const uint32_t *
 // One thread per prime of [first, first + count); the block keeps the wheel
 // row in shared memory.  A warp whose 32 primes all expect under 1/64 hit in
 // the window (p > 64 * nodd * (W + 1)) bounds its searches by the window
-// (modsearch_within): it then skips their last levels with odds of at least
-// one half; a lane alone cannot, as its warp runs as long as its deepest lane.
+// (modsearch_within): they end near the level where the Euclid values fall
+// to p / nodd, six or more levels above W.  Where primes expect more hits
+// the per-level test costs more than the few levels it saves (measured with
+// the bound on every warp expecting under one hit per prime).
 template <typename T, bool F>
 __global__ void __launch_bounds__(256) k_sieve_large_search(const __grid_constant__ LargeArgs a, uint64_t first,
                                                             uint64_t count) {
