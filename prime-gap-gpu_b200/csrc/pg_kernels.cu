@@ -648,7 +648,8 @@ __device__ __forceinline__ void sieve_prime(const LargeArgs &a, const uint32_t *
 // row in shared memory.  A warp whose 32 primes all expect under 1/64 hit in
 // the window (p > 64 * nodd * (W + 1)) bounds its searches by the window
 // (modsearch_within): they end near the level where the Euclid values fall
-// to p / nodd, six or more levels above W.  Where primes expect more hits
+// to p / nodd > 64 (W + 1), about four or more levels (a factor ~3.3 each)
+// before the values reach W.  Where primes expect more hits
 // the per-level test costs more than the few levels it saves (measured with
 // the bound on every warp expecting under one hit per prime).
 template <typename T, bool F>
