@@ -35,3 +35,15 @@ def test_reference_arm_other_ranks_stay_silent():
     r = _run({"WORLD_SIZE": "2", "RANK": "1", "LOCAL_RANK": "1"})
     assert r.returncode == 0, r.stderr[-2000:]
     assert not [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+
+
+def test_roofline_work_per_test():
+    """The limb-product counts behind the bench line's roofline: the fixed formula 2*L^2*(B + ceil(B/5))
+    and the kernel's own work per strong base-2 test (B - 1 squarings of L(L+1)/2 + L^2 + L products)."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    assert bench.products_per_test(703) == 816_992          # P=503: 703-bit N, 22 words
+    assert bench.products_per_test(462) == 249_750          # P=337
+    assert bench.products_per_test(1264) == 4_854_400       # P=907
+    assert bench.kernel_products_per_test(703, 22) == 532_818
+    assert bench.kernel_products_per_test(703, 22) / bench.products_per_test(703) < 0.66
